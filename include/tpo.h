@@ -1,0 +1,171 @@
+/*
+ * tpo.h -- C ABI of libtpo, the sm_100a kernels behind the SIMP
+ * compliance-minimisation loop of tomohiron907/toptimization.
+ *
+ * Plain C types only (pointers, sizes, PODs); no torch types. Every function
+ * returns a tpo_status code, is asynchronous on the given stream unless noted,
+ * never allocates or frees caller buffers, and takes device pointers that the
+ * caller owns (PyTorch tensors in the Python host). Scratch comes from a
+ * caller-provided workspace whose size the matching *_workspace_bytes query
+ * returns; workspaces must be 256-byte aligned and not shared between calls
+ * that may run concurrently.
+ *
+ * Layouts (2D structured Q4 grid, nelx x nely unit elements):
+ *   node (ix, iy)          -> ix*(nely+1) + iy            (iy fastest)
+ *   nodal vector  v        -> v[2*node + {0:x, 1:y}]     (2*(nelx+1)*(nely+1))
+ *   element (ex, ey)       -> ex*nely + ey                (nelx*nely)
+ *   fixed mask             -> uint8 per node, bit0 = x fixed, bit1 = y fixed
+ * These are the reference's numbering (src/toptimization/mesh.py:1-24,
+ * src/toptimization/problem.py:167-173); the fixed mask replaces its int32
+ * per-DOF `is_fixed` field (src/toptimization/fem/fields.py:146-148).
+ */
+#ifndef TPO_H
+#define TPO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *tpo_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+typedef enum tpo_status {
+  TPO_OK = 0,
+  TPO_ERR_ARGS = 1,          /* bad sizes, null or misaligned pointers */
+  TPO_ERR_CUDA = 2,          /* a CUDA call failed; see tpo_last_error_string */
+  TPO_ERR_NOT_CONVERGED = 3, /* not returned by solves: see tpo_solve_result */
+  TPO_ERR_BREAKDOWN = 4,
+  TPO_ERR_NONFINITE = 5,
+  TPO_ERR_TIMEOUT = 6,
+  TPO_ERR_NO_STIFFNESS = 7,  /* tpo_set_stiffness not called on this device */
+  TPO_ERR_WORKSPACE = 8      /* workspace smaller than the query returned */
+} tpo_status;
+
+/* Solve outcome codes (tpo_solve_result.status). */
+enum {
+  TPO_SOLVE_RUNNING = 0,
+  TPO_SOLVE_CONVERGED = 1,
+  TPO_SOLVE_MAX_ITER = 2,
+  TPO_SOLVE_BREAKDOWN = 3,   /* |p.Ap| < 1e-30 (reference solver.py:114-115) */
+  TPO_SOLVE_NONFINITE = 4,
+  TPO_SOLVE_ZERO_RHS = 5     /* ||f|| < 1e-30: u = 0 (reference solver.py:61-63) */
+};
+
+/* Preconditioners. */
+enum {
+  TPO_PRECOND_NONE = 0,
+  TPO_PRECOND_JACOBI = 1,       /* reference "jacobi" (kernels.py:65-101) */
+  TPO_PRECOND_BLOCK_JACOBI = 2, /* reference "block_jacobi": element-block form
+                                   (fem/preconditioner.py:47-108) */
+  TPO_PRECOND_NODAL_BLOCK = 3   /* 2x2 nodal block-Jacobi; no reference counterpart */
+};
+
+/* Solve precisions. */
+enum {
+  TPO_PRECISION_FP64 = 0,  /* plain FP64 PCG */
+  TPO_PRECISION_MIXED = 1  /* FP32 inner PCG inside FP64 iterative refinement */
+};
+
+typedef struct tpo_grid {
+  int32_t nelx, nely;
+  double e_min;    /* SIMP floor: scale = e_min + rho^penalty (1 - e_min) */
+  double penalty;  /* (reference fem/kernels.py:92,160) */
+} tpo_grid;
+
+typedef struct tpo_solve_cfg {
+  int32_t precond;      /* TPO_PRECOND_* */
+  int32_t precision;    /* TPO_PRECISION_* */
+  int32_t max_iter;     /* FP64: PCG iterations; mixed: inner iterations per solve */
+  int32_t warm_start;   /* nonzero: start from u as passed (fixed DOFs zeroed) */
+  double tol;           /* stop when ||r||^2 < (tol*||f||)^2 */
+  double f_norm_sq;     /* ||f||^2, computed once by the caller */
+  double inner_tol;     /* mixed: relative tolerance of each inner solve */
+  int32_t max_outer;    /* mixed: refinement steps */
+  int32_t poll_every;   /* iterations between host checks of the device status
+                           (0 = library default); no effect on results */
+} tpo_solve_cfg;
+
+typedef struct tpo_solve_result {
+  int32_t status;       /* TPO_SOLVE_* */
+  int32_t iters;        /* the reference's count: it+1 on convergence, max_iter
+                           otherwise (also after a breakdown), 0 for zero rhs;
+                           mixed: total inner iterations */
+  int32_t outer_iters;  /* mixed: refinement steps taken (FP64: 1) */
+  int32_t updates;      /* PCG updates actually performed */
+  double rr;            /* last ||r||^2 seen (mixed: true FP64 residual) */
+} tpo_solve_result;
+
+int tpo_version(void);
+const char *tpo_last_error_string(void);
+
+/* Element stiffness (8x8 Q4, row-major), its regularised inverse and the
+ * regulariser (reference fem/fields.py:133-143), copied to constant memory of
+ * the CURRENT device. Must be called once per device before any kernel. */
+int tpo_set_stiffness(const double ke[64], const double ke_inv[64], double alpha_reg);
+
+/* ---- matrix-free K(rho) p --------------------------------------------------
+ * ap = K(rho) p with identity rows at fixed DOFs; *pap_out (device, nullable)
+ * = p.ap. Replaces compute_matvec_2d / matvec_and_dot_2d
+ * (reference fem/kernels.py:143-176, fem/fused_kernels.py:21-56). */
+size_t tpo_matvec_workspace_bytes(const tpo_grid *g);
+int tpo_matvec_f64(const tpo_grid *g, const double *rho, const uint8_t *fixed,
+                   const double *p, double *ap, double *pap_out,
+                   void *ws, size_t ws_bytes, tpo_stream s);
+int tpo_matvec_f32(const tpo_grid *g, const float *rho, const uint8_t *fixed,
+                   const float *p, float *ap, double *pap_out,
+                   void *ws, size_t ws_bytes, tpo_stream s);
+
+/* ---- PCG solve K(rho) u = f ------------------------------------------------
+ * Replaces fem/solver.py:27-159 (host loop + fused kernels) with a
+ * device-resident PCG: alpha/beta/convergence are decided on the GPU; the host
+ * only polls a status word every cfg->poll_every iterations. BLOCKING: returns
+ * when the solve has finished on the device. u holds the warm start on entry
+ * and the solution on exit (the reference's u_prev/u pair). */
+size_t tpo_pcg_workspace_bytes(const tpo_grid *g, const tpo_solve_cfg *c);
+int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c,
+                  const double *rho_phys, const double *f, const uint8_t *fixed,
+                  double *u, void *ws, size_t ws_bytes,
+                  tpo_solve_result *out, tpo_stream s);
+
+/* ---- compliance and sensitivity --------------------------------------------
+ * dc[e] = -p rho^(p-1) (1-e_min) u_e^T Ke u_e; *compliance_out (device) =
+ * sum_e scale_e u_e^T Ke u_e. Replaces compute_sensitivity_2d
+ * (reference fem/kernels.py:234-272). */
+size_t tpo_sensitivity_workspace_bytes(const tpo_grid *g);
+int tpo_sensitivity(const tpo_grid *g, const double *rho_phys, const double *u,
+                    double *dc, double *compliance_out,
+                    void *ws, size_t ws_bytes, tpo_stream s);
+
+/* ---- hat-weight filters ----------------------------------------------------
+ * out[e] = sum_j w_ej x_j / (sum_j w_ej + 1e-20), w = max(0, rmin - dist)
+ * over the in-domain box |dx|,|dy| <= ceil(rmin). Used for both the density
+ * filter and the dc projection (reference optimizer/filter.py:22-149).
+ * scale_out / scale32_out (nullable): SIMP scale of out, FP64 / FP32.
+ * Supports ceil(rmin) <= 16. */
+int tpo_density_filter(const tpo_grid *g, double rmin, const double *x, double *out,
+                       double *scale_out, float *scale32_out, tpo_stream s);
+/* out[e] = sum_j w rho_j dc_j / (rho_e sum_j w + 1e-20)
+ * (reference optimizer/filter.py:152-171). */
+int tpo_sensitivity_filter(const tpo_grid *g, double rmin, const double *rho,
+                           const double *dc, double *out, tpo_stream s);
+
+/* ---- OC update -------------------------------------------------------------
+ * Bisection on lambda in [0, 1e9] (<= 50 steps, stop when
+ * (hi-lo)/(hi+lo+1e-30) < 1e-4), all steps on the device; rho_out = the
+ * update at the last midpoint evaluated (may alias rho_in). result_out
+ * (device, 4 doubles) = {max change, mean(rho_out), last lambda, steps}.
+ * dv may be NULL (all ones). Replaces optimizer/oc.py:21-93 and
+ * fem/kernels.py:330-336. */
+size_t tpo_oc_workspace_bytes(const tpo_grid *g);
+int tpo_oc_update(const tpo_grid *g, double volfrac, double move,
+                  const double *rho_in, const double *dc, const double *dv,
+                  double *rho_out, double *result_out,
+                  void *ws, size_t ws_bytes, tpo_stream s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TPO_H */

@@ -1,0 +1,141 @@
+"""ctypes binding of libtpo (the C ABI in include/tpo.h).
+
+The library is built in-tree (`toptimization_b200/libtpo.so`, see
+`toptimization_b200/csrc/build.py`). There is no fallback: if the library is
+missing or no CUDA device is usable, every device entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_size_t, c_uint8, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(os.environ.get("TPO_LIBRARY", Path(__file__).with_name("libtpo.so")))
+
+TPO_OK = 0
+SOLVE_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "breakdown",
+                4: "nonfinite", 5: "zero_rhs"}
+PRECOND = {"none": 0, "jacobi": 1, "block_jacobi": 2, "nodal_block_jacobi": 3}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+
+class TpoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libtpo error {code}: {msg}")
+        self.code = code
+
+
+class TpoGrid(ctypes.Structure):
+    _fields_ = [("nelx", c_int32), ("nely", c_int32), ("e_min", c_double),
+                ("penalty", c_double)]
+
+
+class TpoSolveCfg(ctypes.Structure):
+    _fields_ = [("precond", c_int32), ("precision", c_int32), ("max_iter", c_int32),
+                ("warm_start", c_int32), ("tol", c_double), ("f_norm_sq", c_double),
+                ("inner_tol", c_double), ("max_outer", c_int32), ("poll_every", c_int32)]
+
+
+class TpoSolveResult(ctypes.Structure):
+    _fields_ = [("status", c_int32), ("iters", c_int32), ("outer_iters", c_int32),
+                ("updates", c_int32), ("rr", c_double)]
+
+
+_PD = POINTER(c_double)
+_SIGS = {
+    "tpo_version": (c_int, []),
+    "tpo_last_error_string": (ctypes.c_char_p, []),
+    "tpo_set_stiffness": (c_int, [_PD, _PD, c_double]),
+    "tpo_matvec_workspace_bytes": (c_size_t, [POINTER(TpoGrid)]),
+    "tpo_matvec_f64": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tpo_matvec_f32": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tpo_pcg_workspace_bytes": (c_size_t, [POINTER(TpoGrid), POINTER(TpoSolveCfg)]),
+    "tpo_pcg_solve": (c_int, [POINTER(TpoGrid), POINTER(TpoSolveCfg), c_void_p, c_void_p,
+                              c_void_p, c_void_p, c_void_p, c_size_t, POINTER(TpoSolveResult),
+                              c_void_p]),
+    "tpo_sensitivity_workspace_bytes": (c_size_t, [POINTER(TpoGrid)]),
+    "tpo_sensitivity": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_size_t, c_void_p]),
+    "tpo_density_filter": (c_int, [POINTER(TpoGrid), c_double, c_void_p, c_void_p, c_void_p,
+                                   c_void_p, c_void_p]),
+    "tpo_sensitivity_filter": (c_int, [POINTER(TpoGrid), c_double, c_void_p, c_void_p,
+                                       c_void_p, c_void_p]),
+    "tpo_oc_workspace_bytes": (c_size_t, [POINTER(TpoGrid)]),
+    "tpo_oc_update": (c_int, [POINTER(TpoGrid), c_double, c_double, c_void_p, c_void_p,
+                              c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def load() -> ctypes.CDLL:
+    """Load libtpo once; raise if it is not built."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise RuntimeError(
+                    f"libtpo not found at {LIB_PATH}; build it with "
+                    "`python -m toptimization_b200.csrc.build` (no CPU fallback exists)")
+            lib = ctypes.CDLL(str(LIB_PATH))
+            for name, (res, args) in _SIGS.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+        return _lib
+
+
+def check(rc: int) -> None:
+    if rc != TPO_OK:
+        msg = load().tpo_last_error_string()
+        raise TpoError(rc, msg.decode() if msg else "")
+
+
+def grid(nelx: int, nely: int, e_min: float, penalty: float) -> TpoGrid:
+    return TpoGrid(int(nelx), int(nely), float(e_min), float(penalty))
+
+
+def ptr(t) -> int:
+    """Device pointer of a torch tensor (0 for None)."""
+    return 0 if t is None else int(t.data_ptr())
+
+
+def stream_handle(stream=None) -> int:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+_stiffness_set: dict[int, bytes] = {}
+
+
+def ensure_stiffness(Ke, Ke_inv, alpha_reg: float) -> None:
+    """Upload Ke (and the element-block inverse) to the current device's
+    constant memory, once per device and matrix."""
+    import numpy as np
+    import torch
+    dev = torch.cuda.current_device()
+    ke = np.ascontiguousarray(Ke, dtype=np.float64).reshape(64)
+    ki = np.ascontiguousarray(Ke_inv, dtype=np.float64).reshape(64)
+    key = ke.tobytes() + ki.tobytes() + np.float64(alpha_reg).tobytes()
+    if _stiffness_set.get(dev) == key:
+        return
+    check(load().tpo_set_stiffness(ke.ctypes.data_as(_PD), ki.ctypes.data_as(_PD),
+                                   c_double(alpha_reg)))
+    _stiffness_set[dev] = key
+
+
+__all__ = ["load", "check", "grid", "ptr", "stream_handle", "ensure_stiffness", "TpoGrid",
+           "TpoSolveCfg", "TpoSolveResult", "TpoError", "PRECOND", "PRECISION", "SOLVE_STATUS",
+           "exported_symbols", "c_float", "c_uint8"]
