@@ -1,0 +1,431 @@
+#!/usr/bin/env python
+"""Benchmark: OC iterations per second of the SIMP loop on the 2048x1024 bridge.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the bridge problem, examples/bridge_2048x1024.yaml): 2048x1024 Q4
+grid (2,097,152 elements, 4,200,450 DOFs), corners pinned, -1/2049 on every
+top node, volfrac 0.3, rmin 4, 2x2 nodal block-Jacobi PCG to 1e-8 warm-started
+from the previous displacement. A step is one OC iteration (density filter,
+PCG solve, sensitivity, dc filter, OC bisection). W untimed steps, then K
+timed steps, each bracketed by CUDA events on the launching stream, with a
+256 MiB write between steps to flush L2. The headline `value` is the mixed
+form (FP32 inner PCG inside FP64 refinement); the plain FP64 form is timed on
+the same steps beside it.
+
+--impl reference times the CPU port of the reference algorithm
+(oracle/csrc/simp_cpu.c, OpenMP on all host cores) on a bounded sample of the
+same workload; the reference's own CPU path is Taichi, which is not available
+in this image.
+
+Multi-GPU (torchrun): every rank solves its own bridge replica (the loop does
+not shard); value = all ranks' OC iterations / the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+WORKLOAD_YAML = REPO / "examples" / "bridge_2048x1024.yaml"
+METRIC = "OC iter/s @2048x1024 mixed vs FP64 at 1e-6 compliance; designs/s, p99 latency"
+UNIT = "OC iter/s"
+PRECONDITIONER = "nodal_block_jacobi"
+# Mean PCG iterations per OC iteration of the plain FP64 bridge solve over OC
+# iterations 4-13 (nodal block-Jacobi, tol 1e-8), measured on B200 by this
+# script (`plain_fp64.cg_iters_mean`). The CPU port runs the same algorithm and
+# reproduces the counts; its bounded sample is scaled to this count.
+FP64_CG_PER_OC = 2000
+CPU_SAMPLE_CG = 48
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="(diagnostics) also print the per-kernel timing pass")
+    return ap.parse_args()
+
+
+def load_workload():
+    from toptimization_b200.problem import load_problem
+    return load_problem(WORKLOAD_YAML)
+
+
+def workload_config(pr, **extra):
+    cfg = {"workload": f"bridge {pr.nelx}x{pr.nely} Q4 (examples/bridge_2048x1024.yaml)",
+           "n_elem": pr.n_elem, "n_dofs": pr.n_dofs, "preconditioner": PRECONDITIONER,
+           "cg_tol": pr.cg_tol, "inner_tol": pr.inner_tol, "volfrac": pr.volfrac,
+           "rmin": pr.rmin, "step": "one OC iteration (filter, PCG, sensitivity, dc filter, OC)",
+           "l2": "flushed between timed steps (256 MiB write)"}
+    cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        power = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(power) if power else None}
+
+
+# ------------------------------------------------------------------ helpers
+def measured_peak():
+    try:
+        peaks = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+        return float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, bf16 copy)"
+    except Exception:
+        return 6650.0, "fallback (6.65 TB/s)"
+
+
+def ncu_traffic(kernel_key: str):
+    """dram bytes per launch of a kernel from the committed ncu summary."""
+    try:
+        data = json.loads((REPO / "profiles" / "traffic.json").read_text())
+        return data.get(kernel_key)
+    except Exception:
+        return None
+
+
+def time_steps(design, steps, warmup, flush_buf, torch):
+    for _ in range(warmup):
+        design.step()
+    torch.cuda.synchronize()
+    times, recs = [], []
+    for _ in range(steps):
+        flush_buf.fill_(1.0)                      # L2 flush, outside the timed interval
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        rec = design.step()
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+        recs.append(rec)
+    return times, recs
+
+
+def time_matvec(pr, dtype, torch, reps=20):
+    """The stiffness operator alone (precomputed scales), L2 flushed between
+    launches, CUDA events around each launch."""
+    import numpy as np
+    from toptimization_b200 import _lib
+    from toptimization_b200.fem import kernels as K
+    from toptimization_b200.mesh import fixed_node_mask
+    g = _lib.grid(pr.nelx, pr.nely, pr.E_min, pr.penalty)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    gen = torch.Generator(device=dev).manual_seed(1)
+    scale = (torch.rand(pr.n_elem, device=dev, generator=gen, dtype=torch.float64) ** 3
+             ).to(dtype)
+    p = torch.randn(pr.n_dofs, device=dev, generator=gen, dtype=torch.float64).to(dtype)
+    ap = torch.empty_like(p)
+    fixed = torch.from_numpy(fixed_node_mask(pr)).to(dev)
+    ws = K.matvec_workspace(g, dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    for _ in range(3):
+        K.apply_stiffness(g, scale, fixed, p, ap, ws)
+    ms = []
+    for _ in range(reps):
+        flush.fill_(2.0)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        K.apply_stiffness(g, scale, fixed, p, ap, ws)
+        b.record()
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    s = np.dtype("float64" if dtype == torch.float64 else "float32").itemsize
+    nbytes = 2 * pr.n_dofs * s + pr.n_elem * s + pr.n_nodes   # p, Ap, scales, mask
+    us = statistics.mean(ms) * 1e3
+    return {"us": round(us, 2), "gbs": round(nbytes / (us * 1e-6) / 1e9, 1),
+            "bytes_per_launch": nbytes, "launches": reps}
+
+
+def cpu_sample(pr, cg_per_oc, steps=1, warm_steps=0):
+    """C/OpenMP port of the reference on the host cores: each sample is one
+    OC iteration with the PCG capped at CPU_SAMPLE_CG iterations; the PCG time
+    is scaled to `cg_per_oc` iterations."""
+    from oracle import simp_cpu
+    cpu = simp_cpu.CpuSimp(pr, preconditioner=PRECONDITIONER)
+    for _ in range(warm_steps):
+        cpu.iteration(max_cg=CPU_SAMPLE_CG)
+    est = []
+    for _ in range(steps):
+        r = cpu.iteration(max_cg=CPU_SAMPLE_CG)
+        per_cg = r["pcg_seconds"] / max(r["cg_iters"], 1)
+        est.append(r["other_seconds"] + per_cg * cg_per_oc)
+    cpu.close()
+    t = sum(est) / len(est)
+    return {"value": round(1.0 / t, 5), "unit": UNIT, "cores": simp_cpu.threads(),
+            "kind": "port",
+            "sample": (f"C/OpenMP port of the reference loop (oracle/csrc/simp_cpu.c, FP64, "
+                       f"{PRECONDITIONER}) on the full 2048x1024 bridge: {steps} OC "
+                       f"iteration(s) with the PCG capped at {CPU_SAMPLE_CG} iterations, "
+                       f"PCG time scaled to {cg_per_oc} iterations per OC iteration"),
+            "seconds_per_oc_iter": round(t, 3)}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pr = load_workload()
+    t0 = time.perf_counter()
+    res = cpu_sample(pr, FP64_CG_PER_OC, steps=args.steps, warm_steps=args.warmup)
+    wall = time.perf_counter() - t0
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 / res["value"], 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(pr, precision="fp64 (CPU port)",
+                                      cg_per_oc_iter=FP64_CG_PER_OC),
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "wall_s": round(wall, 1)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from toptimization_b200 import _lib
+    from toptimization_b200.csrc import build as csrc_build
+    from toptimization_b200.optimizer.simp import SimpDesign, run
+    if rank == 0:
+        csrc_build.build()
+    if world > 1:
+        dist.barrier()
+    lib = _lib.load()
+    dev = torch.device("cuda", local)
+    pr = load_workload()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- mixed (headline), timed
+    mixed = SimpDesign(pr, device=dev, precision="mixed", preconditioner=PRECONDITIONER)
+    for _ in range(args.warmup):
+        mixed.step()
+    barrier()
+    lib.tpo_profile_reset()
+    with ClockSampler(local) as clocks:
+        times_m, recs_m = time_steps(mixed, args.steps, 0, flush, torch)
+    barrier()
+    launches = _lib.profile_read()["launches"]
+    t_mixed = max_over_ranks(sum(times_m))
+    clock_info = clocks.summary()
+
+    # ---- per-kernel timing pass (events around every PCG launch), same design
+    lib.tpo_profile_enable(1)
+    lib.tpo_profile_reset()
+    for _ in range(2):
+        mixed.step()
+    torch.cuda.synchronize()
+    prof = _lib.profile_read()
+    lib.tpo_profile_enable(0)
+    del mixed
+
+    # ---- plain FP64, same steps
+    fp64 = None
+    if not args.no_fp64:
+        d64 = SimpDesign(pr, device=dev, precision="fp64", preconditioner=PRECONDITIONER)
+        for _ in range(args.warmup):
+            d64.step()
+        barrier()
+        times_d, recs_d = time_steps(d64, args.steps, 0, flush, torch)
+        barrier()
+        t_d = max_over_ranks(sum(times_d))
+        cm = np.array([r.compliance for r in recs_m])
+        cd = np.array([r.compliance for r in recs_d])
+        fp64 = {"value": round(world * args.steps / (t_d / 1e3), 4),
+                "ms_per_step": round(t_d / args.steps, 3),
+                "cg_iters_mean": float(np.mean([r.cg_iters for r in recs_d])),
+                "cg_iters": [r.cg_iters for r in recs_d],
+                "compliance": [float(x) for x in cd]}
+        del d64
+
+    # ---- matvec roofline (FP64 and FP32 operator alone)
+    mv64 = time_matvec(pr, torch.float64, torch)
+    mv32 = time_matvec(pr, torch.float32, torch)
+
+    # ---- e2e through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pr_e = load_workload()
+        pr_e.max_iter = args.warmup + args.steps
+        pr_e.preconditioner = PRECONDITIONER
+        got = []
+        barrier()
+        t0 = time.perf_counter()
+        run(pr_e, backend="cuda", live_viz=False, precision="mixed", verbose=False, save=False,
+            viz_callback=lambda rho, it, c, v: got.append(rho.nbytes))
+        torch.cuda.synchronize()
+        t_e = max_over_ranks(time.perf_counter() - t0)
+        n_it = pr_e.max_iter
+        h2d = 8 * pr.n_dofs + pr.n_nodes + 2 * 64 * 8       # f, fixed mask, Ke, Ke_inv
+        e2e = {"value": round(world * n_it / t_e, 4), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d / n_it),
+               "d2h_bytes_per_step": int(np.mean(got)) + 5 * 8,
+               "note": (f"simp.run() from a host Problem to the host density, {n_it} OC "
+                        "iterations from the initial design (setup, H2D of loads and BCs, "
+                        "per-iteration D2H of the density to a viz_callback and of 5 scalars)")}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    value = world * args.steps / (t_mixed / 1e3)
+    peak, peak_kind = measured_peak()
+    # dominant PCG kernel of the timed step (by device time in the timing pass)
+    if prof["dir_ms"] >= prof["update_ms"]:
+        kname, kms, kn, kb = ("k_stencil<float,DIR,nodal> (direction + matvec)",
+                              prof["dir_ms"], prof["dir_launches"], prof["dir_bytes"])
+        tkey = "k_stencil_f32_dir"
+    else:
+        kname, kms, kn, kb = ("k_update<float,nodal> (update + preconditioner)",
+                              prof["update_ms"], prof["update_launches"], prof["update_bytes"])
+        tkey = "k_update_f32"
+    avg_s = kms / max(kn, 1) / 1e3
+    bpl = kb / max(kn, 1)
+    achieved = bpl / avg_s / 1e9 if avg_s > 0 else None
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 3),
+                "traffic": ncu_traffic(tkey), "bytes_per_launch": int(bpl),
+                "avg_launch_us": round(avg_s * 1e6, 2), "launches_timed": kn,
+                "peak_kind": peak_kind,
+                "other_kernel": {"update_us": round(prof["update_ms"] / max(prof["update_launches"], 1) * 1e3, 2),
+                                 "update_gbs": round(prof["update_bytes"] / max(prof["update_ms"], 1e-9) / 1e6, 1),
+                                 "dir_us": round(prof["dir_ms"] / max(prof["dir_launches"], 1) * 1e3, 2),
+                                 "dir_gbs": round(prof["dir_bytes"] / max(prof["dir_ms"], 1e-9) / 1e6, 1)}}
+    mv = {"f64": dict(mv64, frac=round(mv64["gbs"] / peak, 3)),
+          "f32": dict(mv32, frac=round(mv32["gbs"] / peak, 3))}
+
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(t_mixed / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (the bridge problem of examples/bridge_2048x1024.yaml)",
+            "config": workload_config(pr, precision="mixed (FP32 inner PCG, FP64 refinement)",
+                                      oc_iterations_timed=f"{args.warmup + 1}..{args.warmup + args.steps}",
+                                      parallelism="replicas" if world > 1 else "single GPU"),
+            "mixed": {"cg_iters": [r.cg_iters for r in recs_m],
+                      "outer_iters": [r.solve.outer_iters for r in recs_m],
+                      "compliance": [r.compliance for r in recs_m]},
+            "gpu_launches": int(launches), "roofline": roofline, "matvec": mv,
+            "clocks": clock_info}
+    if fp64 is not None:
+        line["plain_fp64"] = fp64
+        line["mixed_over_fp64"] = round(value / fp64["value"], 3)
+        rel = [abs(a - b) / abs(b) for a, b in zip(line["mixed"]["compliance"], fp64["compliance"])]
+        line["compliance_rel_err_mixed_vs_fp64"] = max(rel)
+    if e2e is not None:
+        line["e2e"] = e2e
+    if world == 1 and not args.no_cpu:
+        cg = int(round(fp64["cg_iters_mean"])) if fp64 else FP64_CG_PER_OC
+        line["cpu_baseline"] = cpu_sample(pr, cg)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -117,6 +117,15 @@ int tpo_matvec_f32(const tpo_grid *g, const float *rho, const uint8_t *fixed,
                    const float *p, float *ap, double *pap_out,
                    void *ws, size_t ws_bytes, tpo_stream s);
 
+/* Same operator with the SIMP scales already computed (scale[e] =
+ * e_min + rho_e^p (1 - e_min)): the matvec the PCG applies every iteration. */
+int tpo_apply_stiffness_f64(const tpo_grid *g, const double *scale, const uint8_t *fixed,
+                            const double *p, double *ap, double *pap_out,
+                            void *ws, size_t ws_bytes, tpo_stream s);
+int tpo_apply_stiffness_f32(const tpo_grid *g, const float *scale, const uint8_t *fixed,
+                            const float *p, float *ap, double *pap_out,
+                            void *ws, size_t ws_bytes, tpo_stream s);
+
 /* ---- PCG solve K(rho) u = f ------------------------------------------------
  * Replaces fem/solver.py:27-159 (host loop + fused kernels) with a
  * device-resident PCG: alpha/beta/convergence are decided on the GPU; the host
@@ -163,6 +172,25 @@ int tpo_oc_update(const tpo_grid *g, double volfrac, double move,
                   const double *rho_in, const double *dc, const double *dv,
                   double *rho_out, double *result_out,
                   void *ws, size_t ws_bytes, tpo_stream s);
+
+/* ---- kernel timing (diagnostics) ------------------------------------------
+ * When enabled, tpo_pcg_solve brackets every PCG kernel launch with CUDA
+ * events and accumulates the device time of the launches that did work
+ * (replaces the host timers of the reference's checker/profile_bottleneck.py).
+ * Adds two event records per launch; off by default. */
+typedef struct tpo_profile {
+  int64_t dir_launches;     /* direction + matvec kernel */
+  double dir_ms;
+  int64_t update_launches;  /* update + preconditioner kernel */
+  double update_ms;
+  int64_t dir_bytes;        /* algorithmic bytes moved by those launches */
+  int64_t update_bytes;
+  int64_t launches;         /* every libtpo kernel launch since the last reset
+                               (counted whether or not timing is enabled) */
+} tpo_profile;
+int tpo_profile_enable(int on);
+int tpo_profile_reset(void);
+int tpo_profile_read(tpo_profile *out);
 
 #ifdef __cplusplus
 }

@@ -258,6 +258,9 @@ def main():
     small = str(ref_examples / "cantilever_small.yaml")
     runs = {
         "ref_run_mbb_60x20": (str(REPO / "examples" / "mbb_60x20.yaml"), {}, (1, 10, 50)),
+        "ref_run_mbb_60x20_tight": (str(REPO / "examples" / "mbb_60x20.yaml"),
+                                    {"cg_tol": 1e-12, "max_cg_iter": 5000, "max_iter": 60},
+                                    (1, 10, 30)),
         "ref_run_small_jacobi": (small, {"max_iter": 30, "tol": 0.0}, (1, 10)),
         "ref_run_small_block_jacobi": (small, {"max_iter": 30, "tol": 0.0,
                                                "preconditioner": "block_jacobi"}, (1, 10)),

@@ -44,6 +44,13 @@ class TpoSolveResult(ctypes.Structure):
                 ("updates", c_int32), ("rr", c_double)]
 
 
+class TpoProfile(ctypes.Structure):
+    _fields_ = [("dir_launches", ctypes.c_int64), ("dir_ms", c_double),
+                ("update_launches", ctypes.c_int64), ("update_ms", c_double),
+                ("dir_bytes", ctypes.c_int64), ("update_bytes", ctypes.c_int64),
+                ("launches", ctypes.c_int64)]
+
+
 _PD = POINTER(c_double)
 _SIGS = {
     "tpo_version": (c_int, []),
@@ -54,6 +61,10 @@ _SIGS = {
                                c_void_p, c_void_p, c_size_t, c_void_p]),
     "tpo_matvec_f32": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p, c_void_p,
                                c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tpo_apply_stiffness_f64": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tpo_apply_stiffness_f32": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "tpo_pcg_workspace_bytes": (c_size_t, [POINTER(TpoGrid), POINTER(TpoSolveCfg)]),
     "tpo_pcg_solve": (c_int, [POINTER(TpoGrid), POINTER(TpoSolveCfg), c_void_p, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_size_t, POINTER(TpoSolveResult),
@@ -68,6 +79,9 @@ _SIGS = {
     "tpo_oc_workspace_bytes": (c_size_t, [POINTER(TpoGrid)]),
     "tpo_oc_update": (c_int, [POINTER(TpoGrid), c_double, c_double, c_void_p, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tpo_profile_enable": (c_int, [c_int]),
+    "tpo_profile_reset": (c_int, []),
+    "tpo_profile_read": (c_int, [POINTER(TpoProfile)]),
 }
 
 _lock = threading.Lock()
@@ -134,6 +148,12 @@ def ensure_stiffness(Ke, Ke_inv, alpha_reg: float) -> None:
     check(load().tpo_set_stiffness(ke.ctypes.data_as(_PD), ki.ctypes.data_as(_PD),
                                    c_double(alpha_reg)))
     _stiffness_set[dev] = key
+
+
+def profile_read() -> dict:
+    p = TpoProfile()
+    check(load().tpo_profile_read(p))
+    return {k: getattr(p, k) for k, _ in TpoProfile._fields_}
 
 
 __all__ = ["load", "check", "grid", "ptr", "stream_handle", "ensure_stiffness", "TpoGrid",

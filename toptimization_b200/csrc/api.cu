@@ -11,6 +11,9 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
+#include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 #include "design.cuh"
@@ -48,7 +51,14 @@ int fail(int code, const char *fmt, ...) {
                   __FILE__, __LINE__);                                                    \
   } while (0)
 
-#define TPO_CK_LAUNCH() TPO_CK(cudaGetLastError())
+std::atomic<int64_t> g_launches{0};
+
+// after every kernel launch: count it and surface launch errors
+#define TPO_CK_LAUNCH()        \
+  do {                         \
+    g_launches.fetch_add(1);   \
+    TPO_CK(cudaGetLastError()); \
+  } while (0)
 
 int current_device(int *dev) {
   TPO_CK(cudaGetDevice(dev));
@@ -192,19 +202,49 @@ int get_poller(Poller **out) {
   return TPO_OK;
 }
 
+// ----------------------------------------------------------------- kernel timing
+// Opt-in event timing of the PCG kernels (tpo_profile_*). Four events per
+// iteration slot (direction start/end, update start/end), created lazily.
+constexpr int kProfSlots = 16384;
+bool g_prof_on = false;
+tpo_profile g_prof{};
+std::vector<cudaEvent_t> g_prof_ev[kMaxDevices];
+
+int prof_events(int slots, cudaEvent_t **out) {
+  int dev;
+  int rc = current_device(&dev);
+  if (rc) return rc;
+  std::vector<cudaEvent_t> &v = g_prof_ev[dev];
+  while ((int)v.size() < 4 * slots) {
+    cudaEvent_t e;
+    TPO_CK(cudaEventCreate(&e));
+    v.push_back(e);
+  }
+  *out = v.data();
+  return TPO_OK;
+}
+
+struct LaunchBytes {
+  int64_t dir, update;
+};
+
 // Runs PCG iterations (direction kernel + update kernel) until the device
-// status leaves RUNNING. `iter` enqueues one iteration.
+// status leaves RUNNING. `iter(slot, ev)` enqueues one iteration; when ev is
+// non-null it records ev[0..3] around the two launches.
 template <typename IterFn>
 int run_iterations(IterFn iter, PcgCtl *dctl, int max_iter, int chunk, cudaStream_t st,
-                   PcgCtl *final_out) {
+                   PcgCtl *final_out, LaunchBytes lb) {
   Poller *pl;
   int rc = get_poller(&pl);
   if (rc) return rc;
+  cudaEvent_t *ev = nullptr;
+  const int prof_slots = g_prof_on ? std::min(max_iter, kProfSlots) : 0;
+  if (prof_slots > 0 && (rc = prof_events(prof_slots, &ev))) return rc;
   int issued = 0;
   bool pending[2] = {false, false};
   auto issue = [&](int slot) -> int {
     for (int i = 0; i < chunk && issued < max_iter; ++i, ++issued) {
-      int r = iter();
+      int r = iter(issued, issued < prof_slots ? ev + 4 * issued : nullptr);
       if (r) return r;
     }
     TPO_CK(cudaMemcpyAsync(&pl->host[slot], dctl, sizeof(PcgCtl), cudaMemcpyDeviceToHost, st));
@@ -227,7 +267,35 @@ int run_iterations(IterFn iter, PcgCtl *dctl, int max_iter, int chunk, cudaStrea
   TPO_CK(cudaMemcpyAsync(&pl->host[0], dctl, sizeof(PcgCtl), cudaMemcpyDeviceToHost, st));
   TPO_CK(cudaStreamSynchronize(st));
   *final_out = pl->host[0];
+  if (prof_slots > 0) {
+    // only the launches that did work: the first `it` iterations
+    const int real = std::min(final_out->it, std::min(issued, prof_slots));
+    for (int i = 0; i < real; ++i) {
+      float a = 0.f, b = 0.f;
+      TPO_CK(cudaEventElapsedTime(&a, ev[4 * i], ev[4 * i + 1]));
+      TPO_CK(cudaEventElapsedTime(&b, ev[4 * i + 2], ev[4 * i + 3]));
+      g_prof.dir_ms += a;
+      g_prof.update_ms += b;
+    }
+    g_prof.dir_launches += real;
+    g_prof.update_launches += real;
+    g_prof.dir_bytes += (int64_t)real * lb.dir;
+    g_prof.update_bytes += (int64_t)real * lb.update;
+  }
   return TPO_OK;
+}
+
+template <typename T, int PRE>
+LaunchBytes launch_bytes(const tpo_grid *g) {
+  const int64_t nn = (int64_t)(g->nelx + 1) * (g->nely + 1), nd = 2 * nn;
+  const int64_t ne = (int64_t)g->nelx * g->nely, s = sizeof(T);
+  LaunchBytes lb;
+  lb.dir = 4 * nd * s + ne * s + nn;  // r|z, p_old -> p, Ap; scales; mask
+  if (PRE == TPO_PRECOND_BLOCK_JACOBI)
+    lb.update = 7 * nd * s + ne * s + nn;  // r, Ap, u, p -> u, r', z; weights
+  else
+    lb.update = 6 * nd * s + (PRE == TPO_PRECOND_NONE ? 0 : ne * s) + nn;  // u, r, p, Ap -> u, r
+  return lb;
 }
 
 // ----------------------------------------------------------------- FP64 PCG
@@ -306,20 +374,25 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
   up.part = w.part;
   up.ctl = w.ctl;
 
-  auto iter = [&]() -> int {
+  auto iter = [&](int, cudaEvent_t *ev) -> int {
+    if (ev) TPO_CK(cudaEventRecord(ev[0], st));
     k_stencil<double, M_DIR, PRE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(d);
     TPO_CK_LAUNCH();
+    if (ev) TPO_CK(cudaEventRecord(ev[1], st));
+    if (ev) TPO_CK(cudaEventRecord(ev[2], st));
     if (block) {
       k_blockpre<double, false, kStripL><<<sh.st, ST_THREADS, 0, st>>>(b);
     } else {
       k_update<double, PRE, kStripL><<<sh.up, ST_THREADS, 0, st>>>(up);
     }
     TPO_CK_LAUNCH();
+    if (ev) TPO_CK(cudaEventRecord(ev[3], st));
     return TPO_OK;
   };
   PcgCtl fin;
   const int chunk = c->poll_every > 0 ? c->poll_every : 16;
-  int rc = run_iterations(iter, w.ctl, c->max_iter, chunk, st, &fin);
+  int rc = run_iterations(iter, w.ctl, c->max_iter, chunk, st, &fin,
+                          launch_bytes<double, PRE>(g));
   if (rc) return rc;
   int status = fin.status;
   if (status == TPO_SOLVE_RUNNING) status = TPO_SOLVE_MAX_ITER;  // max_iter <= 0
@@ -405,15 +478,19 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   up.part = w.part;
   up.ctl = w.ctl;
 
-  auto iter = [&]() -> int {
+  auto iter = [&](int, cudaEvent_t *ev) -> int {
+    if (ev) TPO_CK(cudaEventRecord(ev[0], st));
     k_stencil<float, M_DIR, PRE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(d);
     TPO_CK_LAUNCH();
+    if (ev) TPO_CK(cudaEventRecord(ev[1], st));
+    if (ev) TPO_CK(cudaEventRecord(ev[2], st));
     if (block) {
       k_blockpre<float, false, kStripL><<<sh.st, ST_THREADS, 0, st>>>(b);
     } else {
       k_update<float, PRE, kStripL><<<sh.up, ST_THREADS, 0, st>>>(up);
     }
     TPO_CK_LAUNCH();
+    if (ev) TPO_CK(cudaEventRecord(ev[3], st));
     return TPO_OK;
   };
 
@@ -441,7 +518,7 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
       break;
     }
     PcgCtl fin;
-    rc = run_iterations(iter, w.ctl, c->max_iter, chunk, st, &fin);
+    rc = run_iterations(iter, w.ctl, c->max_iter, chunk, st, &fin, launch_bytes<float, PRE>(g));
     if (rc) return rc;
     total_inner += fin.it;
     ++outer_steps;
@@ -501,6 +578,39 @@ static int matvec_impl(const tpo_grid *g, const T *rho, const uint8_t *fixed, co
   return TPO_OK;
 }
 
+template <typename T>
+static int apply_impl(const tpo_grid *g, const T *scale, const uint8_t *fixed, const T *p, T *ap,
+                      double *pap_out, void *ws, size_t ws_bytes, tpo_stream s) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  int dev;
+  if ((rc = need_stiffness(&dev))) return rc;
+  if (!scale || !fixed || !p || !ap || !ws) return fail(TPO_ERR_ARGS, "NULL pointer argument");
+  if (!aligned(p, 2 * sizeof(T)) || !aligned(ap, 2 * sizeof(T)) || !aligned(ws, kAlign))
+    return fail(TPO_ERR_ARGS, "misaligned pointer");
+  if (ws_bytes < tpo_matvec_workspace_bytes(g))
+    return fail(TPO_ERR_WORKSPACE, "workspace too small");
+  const Shapes sh = shapes(g);
+  cudaStream_t st = static_cast<cudaStream_t>(s);
+  Carve cv(ws);
+  PcgCtl *ctl = cv.take<PcgCtl>(1);
+  double *part = cv.take<double>((size_t)sh.nb_max);
+  TPO_CK(cudaMemsetAsync(ctl, 0, sizeof(PcgCtl), st));
+  StArgs a{};
+  a.nx = g->nelx;
+  a.ny = g->nely;
+  a.s = scale;
+  a.fixed = fixed;
+  a.in = p;
+  a.out = ap;
+  a.part = part;
+  a.ctl = ctl;
+  a.result = pap_out;
+  k_stencil<T, M_RAW, TPO_PRECOND_NONE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(a);
+  TPO_CK_LAUNCH();
+  return TPO_OK;
+}
+
 // =================================================================== C ABI
 extern "C" {
 
@@ -546,6 +656,37 @@ int tpo_matvec_f64(const tpo_grid *g, const double *rho, const uint8_t *fixed, c
 int tpo_matvec_f32(const tpo_grid *g, const float *rho, const uint8_t *fixed, const float *p,
                    float *ap, double *pap_out, void *ws, size_t ws_bytes, tpo_stream s) {
   return matvec_impl<float>(g, rho, fixed, p, ap, pap_out, ws, ws_bytes, s);
+}
+
+int tpo_apply_stiffness_f64(const tpo_grid *g, const double *scale, const uint8_t *fixed,
+                            const double *p, double *ap, double *pap_out, void *ws,
+                            size_t ws_bytes, tpo_stream s) {
+  return apply_impl<double>(g, scale, fixed, p, ap, pap_out, ws, ws_bytes, s);
+}
+
+int tpo_apply_stiffness_f32(const tpo_grid *g, const float *scale, const uint8_t *fixed,
+                            const float *p, float *ap, double *pap_out, void *ws,
+                            size_t ws_bytes, tpo_stream s) {
+  return apply_impl<float>(g, scale, fixed, p, ap, pap_out, ws, ws_bytes, s);
+}
+
+// ------------------------------------------------------------------ profiling
+int tpo_profile_enable(int on) {
+  g_prof_on = on != 0;
+  return TPO_OK;
+}
+
+int tpo_profile_reset(void) {
+  g_prof = tpo_profile{};
+  g_launches.store(0);
+  return TPO_OK;
+}
+
+int tpo_profile_read(tpo_profile *out) {
+  if (!out) return fail(TPO_ERR_ARGS, "NULL profile");
+  *out = g_prof;
+  out->launches = g_launches.load();
+  return TPO_OK;
 }
 
 // ------------------------------------------------------------------ PCG

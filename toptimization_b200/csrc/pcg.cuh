@@ -96,37 +96,58 @@ __global__ void __launch_bounds__(ST_THREADS) k_stencil(StArgs a) {
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
 
+  // Raw inputs of one column, fetched one column ahead so that its loads are
+  // in flight while the current column is computed.
+  struct Raw {
+    T sd, su;
+    V2<T> a, b;
+    unsigned m;
+  };
+  auto fetch = [&](int c, Raw &R) {
+    load_elem_col<T>(s, c, y, nx, ny, R.sd, R.su);
+    R.m = 0;
+    R.a = zero2;
+    R.b = zero2;
+    if (row_ok && c >= 0 && c <= nx) {
+      const size_t node = (size_t)c * ny1 + y;
+      R.m = a.fixed[node];
+      if constexpr (MODE == M_DIR) {
+        if constexpr (PRE == TPO_PRECOND_BLOCK_JACOBI) R.a = ld2<T>(static_cast<const T *>(a.z), node);
+        else R.a = ld2<T>(static_cast<const T *>(a.r), node);
+        if (!first) R.b = ld2<T>(src_p, node);
+      } else {
+        R.a = ld2<T>(static_cast<const T *>(a.in), node);
+      }
+    }
+  };
+  Raw nxt;
+  fetch(x0 - 1, nxt);
+
   for (int c = x0 - 1; c <= x1; ++c) {
+    const Raw cur = nxt;
+    if (c < x1) fetch(c + 1, nxt);
     e0d = e1d; e0u = e1u; e1d = e2d; e1u = e2u;
-    load_elem_col<T>(s, c, y, nx, ny, e2d, e2u);
+    e2d = cur.sd;
+    e2u = cur.su;
 
     // ---- transformed nodal value at (c, y)
     V2<T> v = zero2;
-    unsigned m = 0;
+    const unsigned m = cur.m;
     if (row_ok && c >= 0 && c <= nx) {
-      const size_t node = (size_t)c * ny1 + y;
-      m = a.fixed[node];
       if constexpr (MODE == M_RAW) {
-        v = ld2<T>(static_cast<const T *>(a.in), node);
+        v = cur.a;
       } else if constexpr (MODE == M_DIR) {
         V2<T> z;
-        if constexpr (PRE == TPO_PRECOND_BLOCK_JACOBI) {
-          z = ld2<T>(static_cast<const T *>(a.z), node);
-        } else {
-          const V2<T> r = ld2<T>(static_cast<const T *>(a.r), node);
-          z = point_precond<T, PRE>(r, m, e1d, e1u, e2d, e2u);
-        }
-        if (first) {
-          v = z;
-        } else {
-          const V2<T> po = ld2<T>(src_p, node);
-          v = mk2<T>(fmaT(T(beta), po.x, z.x), fmaT(T(beta), po.y, z.y));
-        }
+        if constexpr (PRE == TPO_PRECOND_BLOCK_JACOBI) z = cur.a;
+        else z = point_precond<T, PRE>(cur.a, m, e1d, e1u, e2d, e2u);
+        if (first) v = z;
+        else v = mk2<T>(fmaT(T(beta), cur.b.x, z.x), fmaT(T(beta), cur.b.y, z.y));
       } else {  // M_RES, M_RESX: u with fixed DOFs zeroed (idempotent write-back)
-        v = ld2<T>(static_cast<const T *>(a.in), node);
+        v = cur.a;
         if (m & FIXED_X) v.x = T(0);
         if (m & FIXED_Y) v.y = T(0);
-        if (m && own_row && c >= x0 && c < x1) st2<T>(static_cast<T *>(a.uw), node, v);
+        if (m && own_row && c >= x0 && c < x1)
+          st2<T>(static_cast<T *>(a.uw), (size_t)c * ny1 + y, v);
       }
     }
     n0d = n1d; n0m = n1m; n0u = n1u;
@@ -267,26 +288,51 @@ __global__ void __launch_bounds__(ST_THREADS) k_update(UpdArgs a) {
   T *__restrict__ r = static_cast<T *>(a.r);
   const T *__restrict__ ap = static_cast<const T *>(a.ap);
 
-  T ead = T(0), eau = T(0), ebd = T(0), ebu = T(0);
+  // Columns are processed in batches of UB: all loads of a batch are issued
+  // before any of its arithmetic, so UB columns of loads are in flight.
+  constexpr int UB = 4;
+  T ebd = T(0), ebu = T(0);
   if (PRE != TPO_PRECOND_NONE) load_elem_col<T>(s, x0 - 1, y, nx, ny, ebd, ebu);
   double acc[2] = {0.0, 0.0};
-  for (int c = x0; c < x1; ++c) {
-    ead = ebd; eau = ebu;
-    if (PRE != TPO_PRECOND_NONE) load_elem_col<T>(s, c, y, nx, ny, ebd, ebu);
-    if (row_ok) {
-      const size_t node = (size_t)c * ny1 + y;
-      const unsigned m = a.fixed[node];
-      V2<T> uv = ld2<T>(u, node), rv = ld2<T>(r, node);
-      const V2<T> pv = ld2<T>(p, node), av = ld2<T>(ap, node);
-      uv.x = fmaT(alpha, pv.x, uv.x);
-      uv.y = fmaT(alpha, pv.y, uv.y);
-      rv.x = fmaT(-alpha, av.x, rv.x);
-      rv.y = fmaT(-alpha, av.y, rv.y);
-      st2<T>(u, node, uv);
-      st2<T>(r, node, rv);
-      const V2<T> z = point_precond<T, PRE>(rv, m, ead, eau, ebd, ebu);
-      acc[0] += (double)rv.x * z.x + (double)rv.y * z.y;
-      acc[1] += (double)rv.x * rv.x + (double)rv.y * rv.y;
+  for (int cb = x0; cb < x1; cb += UB) {
+    V2<T> uv[UB], rv[UB], pv[UB], av[UB];
+    T sd[UB], su[UB];
+    unsigned m[UB];
+#pragma unroll
+    for (int k = 0; k < UB; ++k) {
+      const int c = cb + k;
+      sd[k] = su[k] = T(0);
+      m[k] = 0;
+      if (c < x1) {
+        if (PRE != TPO_PRECOND_NONE) load_elem_col<T>(s, c, y, nx, ny, sd[k], su[k]);
+        if (row_ok) {
+          const size_t node = (size_t)c * ny1 + y;
+          m[k] = a.fixed[node];
+          uv[k] = ld2<T>(u, node);
+          rv[k] = ld2<T>(r, node);
+          pv[k] = ld2<T>(p, node);
+          av[k] = ld2<T>(ap, node);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < UB; ++k) {
+      const int c = cb + k;
+      const T ead = ebd, eau = ebu;
+      ebd = sd[k];
+      ebu = su[k];
+      if (c < x1 && row_ok) {
+        const size_t node = (size_t)c * ny1 + y;
+        uv[k].x = fmaT(alpha, pv[k].x, uv[k].x);
+        uv[k].y = fmaT(alpha, pv[k].y, uv[k].y);
+        rv[k].x = fmaT(-alpha, av[k].x, rv[k].x);
+        rv[k].y = fmaT(-alpha, av[k].y, rv[k].y);
+        st2<T>(u, node, uv[k]);
+        st2<T>(r, node, rv[k]);
+        const V2<T> z = point_precond<T, PRE>(rv[k], m[k], ead, eau, ebd, ebu);
+        acc[0] += (double)rv[k].x * z.x + (double)rv[k].y * z.y;
+        acc[1] += (double)rv[k].x * rv[k].x + (double)rv[k].y * rv[k].y;
+      }
     }
   }
   if (!grid_reduce<2>(acc, a.part, &ctl->counter)) return;
@@ -347,24 +393,49 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
   unsigned m1 = 0, m2 = 0;
   double acc[2] = {0.0, 0.0};
 
-  for (int c = x0 - 1; c <= x1; ++c) {
-    e0d = e1d; e0u = e1u;
-    load_elem_col<T>(w, c - 1, y, nx, ny, e1d, e1u);
-    V2<T> rt = zero2, rn = zero2;
-    unsigned m = 0;
+  // raw inputs of column c, fetched one column ahead
+  struct Raw {
+    T wd, wu;
+    V2<T> r, ap, u, p;
+    unsigned m;
+  };
+  auto fetch = [&](int c, Raw &R) {
+    load_elem_col<T>(w, c - 1, y, nx, ny, R.wd, R.wu);
+    R.m = 0;
+    R.r = R.ap = R.u = R.p = zero2;
     if (row_ok && c >= 0 && c <= nx) {
       const size_t node = (size_t)c * ny1 + y;
-      m = a.fixed[node];
-      rn = ld2<T>(r_src, node);
+      R.m = a.fixed[node];
+      R.r = ld2<T>(r_src, node);
       if (!INIT) {
-        const V2<T> av = ld2<T>(ap, node);
-        rn.x = fmaT(-alpha, av.x, rn.x);
-        rn.y = fmaT(-alpha, av.y, rn.y);
+        R.ap = ld2<T>(ap, node);
         if (own_row && c >= x0 && c < x1) {
-          V2<T> uv = ld2<T>(u, node);
-          const V2<T> pv = ld2<T>(p, node);
-          uv.x = fmaT(alpha, pv.x, uv.x);
-          uv.y = fmaT(alpha, pv.y, uv.y);
+          R.u = ld2<T>(u, node);
+          R.p = ld2<T>(p, node);
+        }
+      }
+    }
+  };
+  Raw nxt;
+  fetch(x0 - 1, nxt);
+  for (int c = x0 - 1; c <= x1; ++c) {
+    const Raw cur = nxt;
+    if (c < x1) fetch(c + 1, nxt);
+    e0d = e1d; e0u = e1u;
+    e1d = cur.wd;
+    e1u = cur.wu;
+    V2<T> rt = zero2, rn = zero2;
+    const unsigned m = cur.m;
+    if (row_ok && c >= 0 && c <= nx) {
+      const size_t node = (size_t)c * ny1 + y;
+      rn = cur.r;
+      if (!INIT) {
+        rn.x = fmaT(-alpha, cur.ap.x, rn.x);
+        rn.y = fmaT(-alpha, cur.ap.y, rn.y);
+        if (own_row && c >= x0 && c < x1) {
+          V2<T> uv = cur.u;
+          uv.x = fmaT(alpha, cur.p.x, uv.x);
+          uv.y = fmaT(alpha, cur.p.y, uv.y);
           st2<T>(u, node, uv);
           st2<T>(r_dst, node, rn);
         }

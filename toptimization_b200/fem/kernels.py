@@ -43,6 +43,23 @@ def matvec(grid: _lib.TpoGrid, rho: torch.Tensor, fixed: torch.Tensor, p: torch.
     return (ap, pap) if with_dot else ap
 
 
+def apply_stiffness(grid: _lib.TpoGrid, scale: torch.Tensor, fixed: torch.Tensor,
+                    p: torch.Tensor, ap: torch.Tensor, workspace: torch.Tensor,
+                    pap: torch.Tensor | None = None) -> None:
+    """ap = K p with precomputed element scales (the PCG's operator)."""
+    lib = _lib.load()
+    fn = lib.tpo_apply_stiffness_f64 if p.dtype == torch.float64 else lib.tpo_apply_stiffness_f32
+    if scale.dtype != p.dtype:
+        raise ValueError("scale and p must share a dtype")
+    _lib.check(fn(grid, _lib.ptr(scale), _lib.ptr(fixed), _lib.ptr(p), _lib.ptr(ap),
+                  _lib.ptr(pap), _lib.ptr(workspace), workspace.numel(), _lib.stream_handle()))
+
+
+def matvec_workspace(grid: _lib.TpoGrid, device) -> torch.Tensor:
+    n = _lib.load().tpo_matvec_workspace_bytes(grid)
+    return torch.empty(n, dtype=torch.uint8, device=device)
+
+
 def sensitivity(grid: _lib.TpoGrid, rho_phys: torch.Tensor, u: torch.Tensor,
                 dc: torch.Tensor, compliance: torch.Tensor, workspace: torch.Tensor) -> None:
     """dc = d(compliance)/d(rho_phys); compliance[0] = sum_e scale_e u_e^T Ke u_e."""
