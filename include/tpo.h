@@ -147,6 +147,25 @@ int tpo_sensitivity(const tpo_grid *g, const double *rho_phys, const double *u,
                     double *dc, double *compliance_out,
                     void *ws, size_t ws_bytes, tpo_stream s);
 
+/* Same computation with no workspace argument and no allocation anywhere:
+ * for callers that cannot allocate device memory themselves -- for example a
+ * host whose framework reserves the whole device memory budget up front in
+ * its own pool (a separate cudaMalloc there can fail or fragment the pool),
+ * or a foreign-language binding that only receives finished device buffers
+ * and has no allocator to create a workspace with. No counterpart in the
+ * reference.
+ * Scratch lives in one file-scope device array of TPO_SENS_NOALLOC_SCRATCH
+ * bytes inside libtpo, present on every device that loads the library until
+ * the process exits. Limit: ceil(nely/128) * ceil(nelx/16) <= 32736 (about
+ * 67 million elements); larger grids return TPO_ERR_ARGS. The first call on
+ * a device looks up the array's device address (once per device, with that
+ * device current); make that first call before any stream capture. Every
+ * call reuses the same array, so calls that may overlap on the GPU (other
+ * streams, other threads) race with each other: serialise them. */
+#define TPO_SENS_NOALLOC_SCRATCH (256 * 1024)
+int tpo_sensitivity_noalloc(const tpo_grid *g, const double *rho_phys, const double *u,
+                            double *dc, double *compliance_out, tpo_stream s);
+
 /* ---- hat-weight filters ----------------------------------------------------
  * out[e] = sum_j w_ej x_j / (sum_j w_ej + 1e-20), w = max(0, rmin - dist)
  * over the in-domain box |dx|,|dy| <= ceil(rmin). Used for both the density

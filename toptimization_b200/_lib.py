@@ -72,6 +72,8 @@ _SIGS = {
     "tpo_sensitivity_workspace_bytes": (c_size_t, [POINTER(TpoGrid)]),
     "tpo_sensitivity": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_size_t, c_void_p]),
+    "tpo_sensitivity_noalloc": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p]),
     "tpo_density_filter": (c_int, [POINTER(TpoGrid), c_double, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p]),
     "tpo_sensitivity_filter": (c_int, [POINTER(TpoGrid), c_double, c_void_p, c_void_p,

@@ -778,6 +778,52 @@ int tpo_sensitivity(const tpo_grid *g, const double *rho_phys, const double *u, 
   return TPO_OK;
 }
 
+// ------------------------------------------------------------------ sensitivity, no allocation
+// Scratch for tpo_sensitivity_noalloc: the completion ticket (first 256 bytes)
+// and the per-CTA partial sums. Host code must not take this name as a device
+// address; the address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_sens_scratch[TPO_SENS_NOALLOC_SCRATCH];
+static constexpr size_t kSensTicketBytes = 256;
+static constexpr size_t kSensMaxPartials =
+    (TPO_SENS_NOALLOC_SCRATCH - kSensTicketBytes) / sizeof(double);
+static void *g_sens_scratch_addr[kMaxDevices];
+static std::mutex g_sens_scratch_mu;
+
+int tpo_sensitivity_noalloc(const tpo_grid *g, const double *rho_phys, const double *u,
+                            double *dc, double *compliance_out, tpo_stream s) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  int dev;
+  if ((rc = need_stiffness(&dev))) return rc;
+  if (!rho_phys || !u || !dc || !compliance_out) return fail(TPO_ERR_ARGS, "NULL pointer argument");
+  if (!aligned(u, 16)) return fail(TPO_ERR_ARGS, "misaligned pointer");
+  const dim3 gr((g->nely + S_THREADS - 1) / S_THREADS, (g->nelx + SL - 1) / SL, 1);
+  const size_t nb = (size_t)gr.x * gr.y;
+  if (nb > kSensMaxPartials)
+    return fail(TPO_ERR_ARGS,
+                "grid %dx%d needs %zu partial sums; the fixed scratch holds %zu "
+                "(ceil(nely/128)*ceil(nelx/16) must be <= %zu)",
+                g->nelx, g->nely, nb, kSensMaxPartials, kSensMaxPartials);
+  void *base;
+  {
+    std::lock_guard<std::mutex> lk(g_sens_scratch_mu);
+    if (!g_sens_scratch_addr[dev]) {
+      void *ptr = nullptr;
+      TPO_CK(cudaGetSymbolAddress(&ptr, g_sens_scratch));
+      g_sens_scratch_addr[dev] = ptr;
+    }
+    base = g_sens_scratch_addr[dev];
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(s);
+  SumCtl *ctl = static_cast<SumCtl *>(base);
+  double *part = reinterpret_cast<double *>(static_cast<unsigned char *>(base) + kSensTicketBytes);
+  TPO_CK(cudaMemsetAsync(ctl, 0, sizeof(SumCtl), st));  // the ticket must start at zero
+  k_sensitivity<<<gr, S_THREADS, 0, st>>>(g->nelx, g->nely, g->e_min, g->penalty, rho_phys, u, dc,
+                                          part, ctl, compliance_out);
+  TPO_CK_LAUNCH();
+  return TPO_OK;
+}
+
 // ------------------------------------------------------------------ filters
 static int filter_launch(const tpo_grid *g, double rmin, int mode, const double *x,
                          const double *rho, double *out, double *s_out, float *s32_out,
