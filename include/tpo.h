@@ -206,6 +206,9 @@ typedef struct tpo_profile {
   int64_t update_bytes;
   int64_t launches;         /* every libtpo kernel launch since the last reset
                                (counted whether or not timing is enabled) */
+  int64_t apply_launches;   /* stiffness kernel of tpo_matvec_* / tpo_apply_stiffness_* */
+  double apply_ms;
+  int64_t apply_bytes;
 } tpo_profile;
 int tpo_profile_enable(int on);
 int tpo_profile_reset(void);

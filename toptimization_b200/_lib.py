@@ -48,7 +48,8 @@ class TpoProfile(ctypes.Structure):
     _fields_ = [("dir_launches", ctypes.c_int64), ("dir_ms", c_double),
                 ("update_launches", ctypes.c_int64), ("update_ms", c_double),
                 ("dir_bytes", ctypes.c_int64), ("update_bytes", ctypes.c_int64),
-                ("launches", ctypes.c_int64)]
+                ("launches", ctypes.c_int64), ("apply_launches", ctypes.c_int64),
+                ("apply_ms", c_double), ("apply_bytes", ctypes.c_int64)]
 
 
 _PD = POINTER(c_double)

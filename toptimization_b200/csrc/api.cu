@@ -26,7 +26,6 @@ using namespace tpo;
 namespace {
 
 constexpr int kMaxDevices = 64;
-constexpr int kStripL = 16;            // node columns per stencil thread
 constexpr size_t kAlign = 256;
 
 thread_local std::string g_err;
@@ -74,6 +73,53 @@ int need_stiffness(int *dev) {
   return TPO_OK;
 }
 
+// The bilinear plane-stress Ke of a unit square splits exactly into a centre
+// (one-point) part and a rank-2 hourglass part:
+//   Ke = B0^T D B0 + ch (hx hx^T + hy hy^T),
+//   B0 = strain-displacement matrix at the element centre
+//        (dN/dx = (-1, 1, 1, -1)/2, dN/dy = (-1, -1, 1, 1)/2 per corner),
+//   D  = [[d11, d12, 0], [d12, d11, 0], [0, 0, d33]],  hx, hy = (1, -1, 1, -1)
+//   on the x (y) DOFs of the corners.
+// The stencil applies Ke in that form (about 40 flops per element instead of
+// 64 multiply-adds). The four constants are read off Ke's entries and the
+// decomposition is checked against every entry; a Ke that does not have this
+// structure is rejected. kst = {d11/4, d12/4, d33/4, ch}.
+int stiffness_structure(const double ke[64], double kst[4]) {
+  const double ch = 0.5 * (ke[0] + ke[4]);
+  const double d12 = 2.0 * (ke[1] + ke[3]);
+  const double d33 = 2.0 * (ke[1] - ke[3]);
+  const double d11 = 2.0 * (ke[0] - ke[4]) - d33;
+  const double dnx[4] = {-0.5, 0.5, 0.5, -0.5}, dny[4] = {-0.5, -0.5, 0.5, 0.5};
+  const double h[4] = {1.0, -1.0, 1.0, -1.0};
+  double b[3][8] = {};
+  for (int i = 0; i < 4; ++i) {
+    b[0][2 * i] = dnx[i];
+    b[1][2 * i + 1] = dny[i];
+    b[2][2 * i] = dny[i];
+    b[2][2 * i + 1] = dnx[i];
+  }
+  const double d[3][3] = {{d11, d12, 0.0}, {d12, d11, 0.0}, {0.0, 0.0, d33}};
+  double scale = 0.0, err = 0.0;
+  for (int i = 0; i < 64; ++i) scale = fmax(scale, fabs(ke[i]));
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 8; ++j) {
+      double v = 0.0;
+      for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) v += b[p][i] * d[p][q] * b[q][j];
+      if ((i & 1) == (j & 1)) v += ch * h[i / 2] * h[j / 2];
+      err = fmax(err, fabs(v - ke[8 * i + j]));
+    }
+  if (!(scale > 0.0) || !(err <= 1e-12 * scale))
+    return fail(TPO_ERR_ARGS,
+                "ke is not the bilinear plane-stress element of a unit square "
+                "(structure mismatch %.3e of max entry %.3e)", err, scale);
+  kst[0] = 0.25 * d11;
+  kst[1] = 0.25 * d12;
+  kst[2] = 0.25 * d33;
+  kst[3] = ch;
+  return TPO_OK;
+}
+
 bool aligned(const void *p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
 
 // Bump allocator over the caller's workspace (base == nullptr: size query).
@@ -97,26 +143,7 @@ int check_grid(const tpo_grid *g) {
   return TPO_OK;
 }
 
-// ----------------------------------------------------------------- launch shapes
-struct Shapes {
-  dim3 st, up;      // stencil (30-row warps) and pointwise (32-row warps) grids
-  int nb_max;       // most CTAs of any PCG kernel
-  size_t n_nodes, n_elem;
-};
-
-Shapes shapes(const tpo_grid *g) {
-  Shapes s;
-  const int rows = g->nely + 1, cols = g->nelx + 1;
-  const int warps_y = (rows + ROWS_PER_WARP - 1) / ROWS_PER_WARP;
-  const int wpb = ST_THREADS / 32;
-  s.st = dim3((warps_y + wpb - 1) / wpb, (cols + kStripL - 1) / kStripL, 1);
-  s.up = dim3((rows + ST_THREADS - 1) / ST_THREADS, (cols + kStripL - 1) / kStripL, 1);
-  s.nb_max = (int)std::max(s.st.x * s.st.y, s.up.x * s.up.y);
-  s.n_nodes = (size_t)rows * cols;
-  s.n_elem = (size_t)g->nelx * g->nely;
-  return s;
-}
-
+// ----------------------------------------------------------------- launch plans
 dim3 flat_grid(size_t n, int threads, int cap) {
   size_t b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
@@ -124,51 +151,139 @@ dim3 flat_grid(size_t n, int threads, int cap) {
   return dim3((unsigned)b, 1, 1);
 }
 
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+  }
+  return n;
+}
+
+// Stencil launch configuration per kernel instantiation: dynamic shared
+// memory (set once), resident CTAs per SM, and the strip length that makes
+// the grid close to one full wave.
+template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
+  static constexpr int G = 2;
+  static constexpr int NG = 4;
+  static constexpr int SMEM = TsGeom<T, MODE>::template slot_bytes<G>() * NG;
+  static int resident() {
+    static int occ = -1;
+    if (occ < 0) {
+      auto kern = k_tstencil<T, C, MODE, PRE, G, NG>;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+      int o = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, ST_THREADS, SMEM) !=
+              cudaSuccess || o < 1)
+        o = 1;
+      occ = o;
+    }
+    return occ;
+  }
+  struct Plan {
+    dim3 grid;
+    int L;
+  };
+  static Plan plan(int nx, int ny) {
+    const int rows = (ny + 1 + RPC - 1) / RPC;
+    const int target = sm_count() * resident();
+    int strips = std::max(1, target / rows);
+    int L = std::max(8, (nx + 1 + strips - 1) / strips);
+    strips = (nx + 1 + L - 1) / L;
+    return Plan{dim3(rows, strips, 1), L};
+  }
+  static int launch(cudaStream_t st, const TsArgs &a, int nx, int ny) {
+    const Plan pl = plan(nx, ny);
+    k_tstencil<T, C, MODE, PRE, G, NG><<<pl.grid, ST_THREADS, SMEM, st>>>(a, pl.L);
+    return TPO_OK;
+  }
+  static int max_ctas(int nx, int ny) {
+    const Plan pl = plan(nx, ny);
+    return (int)(pl.grid.x * pl.grid.y);
+  }
+};
+
+struct UpdPlan {
+  dim3 grid;
+  int L;
+};
+UpdPlan update_plan(int nx, int ny) {
+  const int rows = (ny + 1 + UP_THREADS - 1) / UP_THREADS;
+  const int target = sm_count() * 8;
+  int strips = std::max(1, target / rows);
+  int L = std::max(4, (nx + 1 + strips - 1) / strips);
+  strips = (nx + 1 + L - 1) / L;
+  return UpdPlan{dim3(rows, strips, 1), L};
+}
+constexpr int kBlkL = 16;
+dim3 blk_grid(int nx, int ny) {
+  const int warps_y = (ny + 1 + RPW - 1) / RPW;
+  return dim3((warps_y + WPC - 1) / WPC, (nx + 1 + kBlkL - 1) / kBlkL, 1);
+}
+
+// most CTAs any PCG kernel of this grid can have (sizes the partials buffer)
+int max_ctas(const tpo_grid *g) {
+  const int nx = g->nelx, ny = g->nely;
+  int m = (int)(update_plan(nx, ny).grid.x * update_plan(nx, ny).grid.y);
+  const dim3 bg = blk_grid(nx, ny);
+  m = std::max(m, (int)(bg.x * bg.y));
+  // the stencil plans target at most sm_count * 8 CTAs (resident <= 8 with 128 threads
+  // and >= 37 KB of shared memory); bound generously without querying every variant
+  const int rows = (ny + 1 + RPC - 1) / RPC;
+  m = std::max(m, rows * std::max(1, (nx + 1 + 7) / 8));
+  return m;
+}
+
 // ----------------------------------------------------------------- workspace layout
 struct PcgWs {
   PcgCtl *ctl;
   OuterCtl *octl;
   double *part;
-  double *s64;
-  float *s32;
-  double *w64;
-  float *w32;
-  // FP64 solve vectors
-  double *ra, *rb, *pa, *pb, *ap, *z;
-  // FP32 inner vectors (mixed)
-  float *fra, *frb, *fpa, *fpb, *fap, *fz, *fd;
+  uint8_t *mask;
+  double *u, *f;          // padded FP64 solution and load
+  double *s64, *w64;
+  float *s32, *w32;
+  double *ra, *rb, *pa, *pb, *ap, *z;          // FP64 solve
+  float *fra, *frb, *fpa, *fpb, *fap, *fz, *fy;  // mixed inner solve
+  int P;
   size_t bytes;
 };
 
 PcgWs carve_pcg(void *base, const tpo_grid *g, const tpo_solve_cfg *c) {
-  const Shapes sh = shapes(g);
-  const size_t N = 2 * sh.n_nodes, E = sh.n_elem;
+  const int nx = g->nelx, ny = g->nely, P = pad_pitch(ny);
+  const size_t NN = (size_t)(nx + 1) * P, NE = (size_t)nx * P;
   const bool block = c->precond == TPO_PRECOND_BLOCK_JACOBI;
   const bool mixed = c->precision == TPO_PRECISION_MIXED;
   Carve cv(base);
   PcgWs w{};
+  w.P = P;
   w.ctl = cv.take<PcgCtl>(1);
   w.octl = cv.take<OuterCtl>(1);
-  w.part = cv.take<double>(3 * (size_t)sh.nb_max);
-  w.s64 = cv.take<double>(E);
+  w.part = cv.take<double>(3 * (size_t)max_ctas(g));
+  w.mask = cv.take<uint8_t>(NN);
+  w.u = cv.take<double>(2 * NN);
+  w.f = cv.take<double>(2 * NN);
+  w.s64 = cv.take<double>(NE);
   if (mixed) {
-    w.s32 = cv.take<float>(E);
-    if (block) w.w32 = cv.take<float>(E);
-    w.fra = cv.take<float>(N);
-    if (block) w.frb = cv.take<float>(N);
-    w.fpa = cv.take<float>(N);
-    w.fpb = cv.take<float>(N);
-    w.fap = cv.take<float>(N);
-    if (block) w.fz = cv.take<float>(N);
-    w.fd = cv.take<float>(N);
+    w.s32 = cv.take<float>(NE);
+    if (block) w.w32 = cv.take<float>(NE);
+    w.fra = cv.take<float>(2 * NN);
+    if (block) w.frb = cv.take<float>(2 * NN);
+    w.fpa = cv.take<float>(2 * NN);
+    w.fpb = cv.take<float>(2 * NN);
+    w.fap = cv.take<float>(2 * NN);
+    if (block) w.fz = cv.take<float>(2 * NN);
+    w.fy = cv.take<float>(2 * NN);
   } else {
-    if (block) w.w64 = cv.take<double>(E);
-    w.ra = cv.take<double>(N);
-    if (block) w.rb = cv.take<double>(N);
-    w.pa = cv.take<double>(N);
-    w.pb = cv.take<double>(N);
-    w.ap = cv.take<double>(N);
-    if (block) w.z = cv.take<double>(N);
+    if (block) w.w64 = cv.take<double>(NE);
+    w.ra = cv.take<double>(2 * NN);
+    if (block) w.rb = cv.take<double>(2 * NN);
+    w.pa = cv.take<double>(2 * NN);
+    w.pb = cv.take<double>(2 * NN);
+    w.ap = cv.take<double>(2 * NN);
+    if (block) w.z = cv.take<double>(2 * NN);
   }
   w.bytes = cv.off;
   return w;
@@ -229,22 +344,24 @@ struct LaunchBytes {
 };
 
 // Runs PCG iterations (direction kernel + update kernel) until the device
-// status leaves RUNNING. `iter(slot, ev)` enqueues one iteration; when ev is
-// non-null it records ev[0..3] around the two launches.
+// status leaves RUNNING. `iter(ev)` enqueues one iteration; when ev is
+// non-null it records ev[0..3] around the two launches. it0 = the device
+// iteration count when this call starts.
 template <typename IterFn>
-int run_iterations(IterFn iter, PcgCtl *dctl, int max_iter, int chunk, cudaStream_t st,
+int run_iterations(IterFn iter, PcgCtl *dctl, int max_iter, int it0, int chunk, cudaStream_t st,
                    PcgCtl *final_out, LaunchBytes lb) {
   Poller *pl;
   int rc = get_poller(&pl);
   if (rc) return rc;
   cudaEvent_t *ev = nullptr;
-  const int prof_slots = g_prof_on ? std::min(max_iter, kProfSlots) : 0;
+  const int budget = std::max(0, max_iter - it0);
+  const int prof_slots = g_prof_on ? std::min(budget, kProfSlots) : 0;
   if (prof_slots > 0 && (rc = prof_events(prof_slots, &ev))) return rc;
   int issued = 0;
   bool pending[2] = {false, false};
   auto issue = [&](int slot) -> int {
-    for (int i = 0; i < chunk && issued < max_iter; ++i, ++issued) {
-      int r = iter(issued, issued < prof_slots ? ev + 4 * issued : nullptr);
+    for (int i = 0; i < chunk && issued < budget; ++i, ++issued) {
+      int r = iter(issued < prof_slots ? ev + 4 * issued : nullptr);
       if (r) return r;
     }
     TPO_CK(cudaMemcpyAsync(&pl->host[slot], dctl, sizeof(PcgCtl), cudaMemcpyDeviceToHost, st));
@@ -252,24 +369,25 @@ int run_iterations(IterFn iter, PcgCtl *dctl, int max_iter, int chunk, cudaStrea
     pending[slot] = true;
     return TPO_OK;
   };
-  if (max_iter > 0) {
+  if (budget > 0) {
     if ((rc = issue(0))) return rc;
-    if (issued < max_iter && (rc = issue(1))) return rc;
+    if (issued < budget && (rc = issue(1))) return rc;
     int cur = 0;
     while (pending[cur]) {
       TPO_CK(cudaEventSynchronize(pl->ev[cur]));
       pending[cur] = false;
-      if (pl->host[cur].status != TPO_SOLVE_RUNNING) break;
-      if (issued < max_iter && (rc = issue(cur))) return rc;
+      if (pl->host[cur].status != TPO_SOLVE_RUNNING || pl->host[cur].err) break;
+      if (issued < budget && (rc = issue(cur))) return rc;
       cur ^= 1;
     }
   }
   TPO_CK(cudaMemcpyAsync(&pl->host[0], dctl, sizeof(PcgCtl), cudaMemcpyDeviceToHost, st));
   TPO_CK(cudaStreamSynchronize(st));
   *final_out = pl->host[0];
+  if (final_out->err) return fail(TPO_ERR_TIMEOUT, "a TMA pipeline wait ran out of time");
   if (prof_slots > 0) {
-    // only the launches that did work: the first `it` iterations
-    const int real = std::min(final_out->it, std::min(issued, prof_slots));
+    // only the launches that did work
+    const int real = std::min(final_out->it - it0, std::min(issued, prof_slots));
     for (int i = 0; i < real; ++i) {
       float a = 0.f, b = 0.f;
       TPO_CK(cudaEventElapsedTime(&a, ev[4 * i], ev[4 * i + 1]));
@@ -277,14 +395,17 @@ int run_iterations(IterFn iter, PcgCtl *dctl, int max_iter, int chunk, cudaStrea
       g_prof.dir_ms += a;
       g_prof.update_ms += b;
     }
-    g_prof.dir_launches += real;
-    g_prof.update_launches += real;
-    g_prof.dir_bytes += (int64_t)real * lb.dir;
-    g_prof.update_bytes += (int64_t)real * lb.update;
+    if (real > 0) {
+      g_prof.dir_launches += real;
+      g_prof.update_launches += real;
+      g_prof.dir_bytes += (int64_t)real * lb.dir;
+      g_prof.update_bytes += (int64_t)real * lb.update;
+    }
   }
   return TPO_OK;
 }
 
+// Algorithmic bytes per launch (compact sizes: N DOFs, E elements, Nn nodes)
 template <typename T, int PRE>
 LaunchBytes launch_bytes(const tpo_grid *g) {
   const int64_t nn = (int64_t)(g->nelx + 1) * (g->nely + 1), nd = 2 * nn;
@@ -298,44 +419,86 @@ LaunchBytes launch_bytes(const tpo_grid *g) {
   return lb;
 }
 
+int pack_inputs(const tpo_grid *g, const PcgWs &w, const double *f, const uint8_t *fixed,
+                const double *u, bool warm, cudaStream_t st) {
+  const int nx = g->nelx, ny = g->nely, P = w.P;
+  const size_t NN = (size_t)(nx + 1) * P;
+  const dim3 fg = flat_grid(NN, 256, sm_count() * 16);
+  k_pack_mask<<<fg, 256, 0, st>>>(nx, ny, P, fixed, w.mask);
+  TPO_CK_LAUNCH();
+  k_pack_nodes<double><<<fg, 256, 0, st>>>(nx, ny, P, f, w.f);
+  TPO_CK_LAUNCH();
+  if (warm) {
+    k_pack_nodes<double><<<fg, 256, 0, st>>>(nx, ny, P, u, w.u);
+    TPO_CK_LAUNCH();
+  } else {
+    TPO_CK(cudaMemsetAsync(w.u, 0, 2 * NN * sizeof(double), st));
+  }
+  return TPO_OK;
+}
+
+// Zero every PCG vector once per solve: the kernels write only grid rows, so
+// the pad slots (which the stencils read as zero neighbours) stay zero.
+int zero_vectors(const PcgWs &w, size_t NN, cudaStream_t st) {
+  double *d64[] = {w.ra, w.rb, w.pa, w.pb, w.ap, w.z};
+  for (double *p : d64)
+    if (p) TPO_CK(cudaMemsetAsync(p, 0, 2 * NN * sizeof(double), st));
+  float *d32[] = {w.fra, w.frb, w.fpa, w.fpb, w.fap, w.fz, w.fy};
+  for (float *p : d32)
+    if (p) TPO_CK(cudaMemsetAsync(p, 0, 2 * NN * sizeof(float), st));
+  return TPO_OK;
+}
+
+int unpack_solution(const tpo_grid *g, const PcgWs &w, double *u, cudaStream_t st) {
+  const size_t n = (size_t)(g->nelx + 1) * (g->nely + 1);
+  k_unpack_nodes<<<flat_grid(n, 256, sm_count() * 16), 256, 0, st>>>(g->nelx, g->nely, w.P, w.u,
+                                                                      u);
+  TPO_CK_LAUNCH();
+  return TPO_OK;
+}
+
 // ----------------------------------------------------------------- FP64 PCG
 template <int PRE>
 int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const double *f,
              const uint8_t *fixed, double *u, const PcgWs &w, tpo_solve_result *out,
              cudaStream_t st, double alpha_reg) {
-  const Shapes sh = shapes(g);
-  const int E = (int)sh.n_elem;
+  const int nx = g->nelx, ny = g->nely, P = w.P;
   constexpr bool block = PRE == TPO_PRECOND_BLOCK_JACOBI;
-  const double tol_sq = (c->tol * std::sqrt(c->f_norm_sq)) * (c->tol * std::sqrt(c->f_norm_sq));
-
-  k_scales<<<flat_grid(E, 256, 148 * 16), 256, 0, st>>>(E, rho, g->e_min, g->penalty, alpha_reg,
-                                                         w.s64, nullptr, block ? w.w64 : nullptr,
-                                                         nullptr);
+  const double fn = std::sqrt(c->f_norm_sq);
+  const double tol_sq = (c->tol * fn) * (c->tol * fn);
+  int rc = pack_inputs(g, w, f, fixed, u, c->warm_start != 0, st);
+  if (rc) return rc;
+  if ((rc = zero_vectors(w, (size_t)(nx + 1) * P, st))) return rc;
+  k_scales<<<flat_grid((size_t)nx * P, 256, sm_count() * 16), 256, 0, st>>>(
+      nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, nullptr, block ? w.w64 : nullptr,
+      nullptr);
   TPO_CK_LAUNCH();
   k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, 0.0, c->max_iter, nullptr, 0.0);
   TPO_CK_LAUNCH();
-  if (!c->warm_start) TPO_CK(cudaMemsetAsync(u, 0, 2 * sh.n_nodes * sizeof(double), st));
 
-  StArgs a{};
-  a.nx = g->nelx;
-  a.ny = g->nely;
+  TsArgs a{};
+  a.nx = nx;
+  a.ny = ny;
+  a.P = P;
   a.s = w.s64;
-  a.fixed = fixed;
-  a.in = u;
-  a.uw = u;
-  a.f = f;
+  a.mask = w.mask;
+  a.a = w.u;
+  a.uw = w.u;
+  a.f = w.f;
   a.out = w.ra;
   a.part = w.part;
   a.ctl = w.ctl;
-  k_stencil<double, M_RES, PRE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(a);
+  a.err = &w.ctl->err;
+  StencilCfg<double, double, M_RES, PRE>::launch(st, a, nx, ny);
   TPO_CK_LAUNCH();
 
   BlkArgs b{};
-  b.nx = g->nelx;
-  b.ny = g->nely;
+  b.nx = nx;
+  b.ny = ny;
+  b.P = P;
   b.w = w.w64;
-  b.fixed = fixed;
-  b.u = u;
+  b.mask = w.mask;
+  b.u = w.u;
   b.ap = w.ap;
   b.pa = w.pa;
   b.pb = w.pb;
@@ -345,45 +508,48 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
   b.part = w.part;
   b.ctl = w.ctl;
   if (block) {
-    k_blockpre<double, true, kStripL><<<sh.st, ST_THREADS, 0, st>>>(b);
+    k_blockpre<double, double, true, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     TPO_CK_LAUNCH();
   }
 
-  StArgs d{};
-  d.nx = g->nelx;
-  d.ny = g->nely;
+  TsArgs d{};
+  d.nx = nx;
+  d.ny = ny;
+  d.P = P;
   d.s = w.s64;
-  d.fixed = fixed;
-  d.out = w.ap;
-  d.r = w.ra;
-  d.z = w.z;
+  d.mask = w.mask;
+  d.a = block ? (const void *)w.z : (const void *)w.ra;
   d.pa = w.pa;
   d.pb = w.pb;
+  d.out = w.ap;
   d.part = w.part;
   d.ctl = w.ctl;
+  d.err = &w.ctl->err;
   UpdArgs up{};
-  up.nx = g->nelx;
-  up.ny = g->nely;
+  up.nx = nx;
+  up.ny = ny;
+  up.P = P;
   up.s = w.s64;
-  up.fixed = fixed;
-  up.u = u;
+  up.mask = w.mask;
+  up.u = w.u;
   up.r = w.ra;
   up.ap = w.ap;
   up.pa = w.pa;
   up.pb = w.pb;
   up.part = w.part;
   up.ctl = w.ctl;
+  const UpdPlan upl = update_plan(nx, ny);
 
-  auto iter = [&](int, cudaEvent_t *ev) -> int {
+  auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
-    k_stencil<double, M_DIR, PRE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(d);
+    StencilCfg<double, double, M_DIR, PRE>::launch(st, d, nx, ny);
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
     if (block) {
-      k_blockpre<double, false, kStripL><<<sh.st, ST_THREADS, 0, st>>>(b);
+      k_blockpre<double, double, false, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     } else {
-      k_update<double, PRE, kStripL><<<sh.up, ST_THREADS, 0, st>>>(up);
+      k_update<double, double, PRE><<<upl.grid, UP_THREADS, 0, st>>>(up, upl.L);
     }
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
@@ -391,9 +557,10 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
   };
   PcgCtl fin;
   const int chunk = c->poll_every > 0 ? c->poll_every : 16;
-  int rc = run_iterations(iter, w.ctl, c->max_iter, chunk, st, &fin,
-                          launch_bytes<double, PRE>(g));
+  rc = run_iterations(iter, w.ctl, c->max_iter, 0, chunk, st, &fin, launch_bytes<double, PRE>(g));
   if (rc) return rc;
+  if ((rc = unpack_solution(g, w, u, st))) return rc;
+  TPO_CK(cudaStreamSynchronize(st));
   int status = fin.status;
   if (status == TPO_SOLVE_RUNNING) status = TPO_SOLVE_MAX_ITER;  // max_iter <= 0
   out->status = status;
@@ -405,45 +572,53 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
 }
 
 // ----------------------------------------------------------------- mixed PCG
+// One FP32-storage PCG (FP64 arithmetic and dot products) whose recursive
+// residual is replaced by the true FP64 residual f - K u whenever it has
+// dropped by inner_tol since the last replacement ("reliable updates"); the
+// search direction is kept across replacements, so the Krylov space is not
+// discarded. Convergence is decided only on the FP64 residual.
 template <int PRE>
 int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const double *f,
               const uint8_t *fixed, double *u, const PcgWs &w, tpo_solve_result *out,
               cudaStream_t st, double alpha_reg) {
-  const Shapes sh = shapes(g);
-  const int E = (int)sh.n_elem;
+  const int nx = g->nelx, ny = g->nely, P = w.P;
+  const size_t NN = (size_t)(nx + 1) * P;
   constexpr bool block = PRE == TPO_PRECOND_BLOCK_JACOBI;
   const double fn = std::sqrt(c->f_norm_sq);
   const double tol_sq = (c->tol * fn) * (c->tol * fn);
-
-  k_scales<<<flat_grid(E, 256, 148 * 16), 256, 0, st>>>(E, rho, g->e_min, g->penalty, alpha_reg,
-                                                         w.s64, w.s32, nullptr,
-                                                         block ? w.w32 : nullptr);
+  const double delta = c->inner_tol > 0.0 ? c->inner_tol : 1e-3;
+  int rc = pack_inputs(g, w, f, fixed, u, c->warm_start != 0, st);
+  if (rc) return rc;
+  if ((rc = zero_vectors(w, NN, st))) return rc;
+  k_scales<<<flat_grid((size_t)nx * P, 256, sm_count() * 16), 256, 0, st>>>(
+      nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, w.s32, nullptr,
+      block ? w.w32 : nullptr);
   TPO_CK_LAUNCH();
-  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, 0.0, c->inner_tol * c->inner_tol, c->max_iter, w.octl,
-                              tol_sq);
+  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, delta * delta, c->max_iter, w.octl, tol_sq);
   TPO_CK_LAUNCH();
-  if (!c->warm_start) TPO_CK(cudaMemsetAsync(u, 0, 2 * sh.n_nodes * sizeof(double), st));
 
-  StArgs rx{};
-  rx.nx = g->nelx;
-  rx.ny = g->nely;
+  TsArgs rx{};
+  rx.nx = nx;
+  rx.ny = ny;
+  rx.P = P;
   rx.s = w.s64;
-  rx.fixed = fixed;
-  rx.in = u;
-  rx.uw = u;
-  rx.f = f;
-  rx.out = w.fra;
-  rx.d = w.fd;
+  rx.mask = w.mask;
+  rx.a = w.u;
+  rx.uw = w.u;
+  rx.f = w.f;
+  rx.d = w.fy;
   rx.part = w.part;
   rx.ctl = w.ctl;
   rx.octl = w.octl;
+  rx.err = &w.ctl->err;
 
   BlkArgs b{};
-  b.nx = g->nelx;
-  b.ny = g->nely;
+  b.nx = nx;
+  b.ny = ny;
+  b.P = P;
   b.w = w.w32;
-  b.fixed = fixed;
-  b.u = w.fd;
+  b.mask = w.mask;
+  b.u = w.fy;
   b.ap = w.fap;
   b.pa = w.fpa;
   b.pb = w.fpb;
@@ -453,41 +628,44 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   b.part = w.part;
   b.ctl = w.ctl;
 
-  StArgs d{};
-  d.nx = g->nelx;
-  d.ny = g->nely;
+  TsArgs d{};
+  d.nx = nx;
+  d.ny = ny;
+  d.P = P;
   d.s = w.s32;
-  d.fixed = fixed;
-  d.out = w.fap;
-  d.r = w.fra;
-  d.z = w.fz;
+  d.mask = w.mask;
+  d.a = block ? (const void *)w.fz : (const void *)w.fra;
   d.pa = w.fpa;
   d.pb = w.fpb;
+  d.out = w.fap;
   d.part = w.part;
   d.ctl = w.ctl;
+  d.err = &w.ctl->err;
   UpdArgs up{};
-  up.nx = g->nelx;
-  up.ny = g->nely;
+  up.nx = nx;
+  up.ny = ny;
+  up.P = P;
   up.s = w.s32;
-  up.fixed = fixed;
-  up.u = w.fd;
+  up.mask = w.mask;
+  up.u = w.fy;
   up.r = w.fra;
   up.ap = w.fap;
   up.pa = w.fpa;
   up.pb = w.fpb;
   up.part = w.part;
   up.ctl = w.ctl;
+  const UpdPlan upl = update_plan(nx, ny);
 
-  auto iter = [&](int, cudaEvent_t *ev) -> int {
+  auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
-    k_stencil<float, M_DIR, PRE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(d);
+    StencilCfg<float, double, M_DIR, PRE>::launch(st, d, nx, ny);
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
     if (block) {
-      k_blockpre<float, false, kStripL><<<sh.st, ST_THREADS, 0, st>>>(b);
+      k_blockpre<float, double, false, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     } else {
-      k_update<float, PRE, kStripL><<<sh.up, ST_THREADS, 0, st>>>(up);
+      k_update<float, double, PRE><<<upl.grid, UP_THREADS, 0, st>>>(up, upl.L);
     }
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
@@ -495,16 +673,23 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   };
 
   Poller *pl;
-  int rc = get_poller(&pl);
-  if (rc) return rc;
-  OuterCtl oh{};
-  int total_inner = 0, outer_steps = 0, status = TPO_SOLVE_MAX_ITER;
+  if ((rc = get_poller(&pl))) return rc;
   const int chunk = c->poll_every > 0 ? c->poll_every : 16;
+  const dim3 fg = flat_grid(2 * NN, 256, sm_count() * 16);
+  OuterCtl oh{};
+  PcgCtl fin{};
+  int status = TPO_SOLVE_MAX_ITER, inner_it = 0;
   for (int k = 0;; ++k) {
-    k_stencil<double, M_RESX, PRE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(rx);
+    if (k > 0) {  // fold the FP32 correction into u before the FP64 residual
+      k_accumulate<<<fg, 256, 0, st>>>(2 * NN, w.u, w.fy);
+      TPO_CK_LAUNCH();
+    }
+    // block preconditioner: the current residual buffer follows the iteration parity
+    rx.out = (block && (inner_it & 1)) ? (void *)w.frb : (void *)w.fra;
+    StencilCfg<double, double, M_RESX, PRE>::launch(st, rx, nx, ny);
     TPO_CK_LAUNCH();
     if (block) {
-      k_blockpre<float, true, kStripL><<<sh.st, ST_THREADS, 0, st>>>(b);
+      k_blockpre<float, double, true, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
       TPO_CK_LAUNCH();
     }
     TPO_CK(cudaMemcpyAsync(&oh, w.octl, sizeof(OuterCtl), cudaMemcpyDeviceToHost, st));
@@ -513,100 +698,101 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
       status = oh.status;
       break;
     }
-    if (k >= c->max_outer) {
+    if (k > 0 && fin.status != SOLVE_NEED_UPDATE) {
+      status = fin.status;  // inner solve stopped (max_iter, breakdown): report it
+      break;
+    }
+    if (oh.it > c->max_outer) {
       status = TPO_SOLVE_MAX_ITER;
       break;
     }
-    PcgCtl fin;
-    rc = run_iterations(iter, w.ctl, c->max_iter, chunk, st, &fin, launch_bytes<float, PRE>(g));
+    rc = run_iterations(iter, w.ctl, c->max_iter, inner_it, chunk, st, &fin,
+                        launch_bytes<float, PRE>(g));
     if (rc) return rc;
-    total_inner += fin.it;
-    ++outer_steps;
+    inner_it = fin.it;
     if (fin.status == TPO_SOLVE_NONFINITE) {
       status = TPO_SOLVE_NONFINITE;
       break;
     }
-    k_correct<<<flat_grid(2 * sh.n_nodes, 256, 148 * 16), 256, 0, st>>>(2 * sh.n_nodes, u, w.fd);
-    TPO_CK_LAUNCH();
+    if (fin.status == TPO_SOLVE_RUNNING) fin.status = TPO_SOLVE_MAX_ITER;
   }
+  if ((rc = unpack_solution(g, w, u, st))) return rc;
   TPO_CK(cudaStreamSynchronize(st));
   out->status = status;
-  out->iters = total_inner;
-  out->updates = total_inner;
-  out->outer_iters = outer_steps;
+  out->iters = inner_it;
+  out->updates = inner_it;
+  out->outer_iters = oh.it;
   out->rr = oh.rr;
   return TPO_OK;
 }
 
-
 }  // namespace
 
-template <typename T>
-static int matvec_impl(const tpo_grid *g, const T *rho, const uint8_t *fixed, const T *p, T *ap,
-                       double *pap_out, void *ws, size_t ws_bytes, tpo_stream s) {
+// ------------------------------------------------------------------ matvec (packing)
+template <typename T, typename C>
+static int apply_impl(const tpo_grid *g, const T *elem, bool from_density, const uint8_t *fixed,
+                      const T *p, T *ap, double *pap_out, void *ws, size_t ws_bytes,
+                      tpo_stream s) {
   int rc = check_grid(g);
   if (rc) return rc;
   int dev;
   if ((rc = need_stiffness(&dev))) return rc;
-  if (!rho || !fixed || !p || !ap || !ws) return fail(TPO_ERR_ARGS, "NULL pointer argument");
+  if (!elem || !fixed || !p || !ap || !ws) return fail(TPO_ERR_ARGS, "NULL pointer argument");
   if (!aligned(p, 2 * sizeof(T)) || !aligned(ap, 2 * sizeof(T)) || !aligned(ws, kAlign))
     return fail(TPO_ERR_ARGS, "misaligned pointer");
   if (ws_bytes < tpo_matvec_workspace_bytes(g))
     return fail(TPO_ERR_WORKSPACE, "workspace too small");
-  const Shapes sh = shapes(g);
+  const int nx = g->nelx, ny = g->nely, P = pad_pitch(ny);
+  const size_t NN = (size_t)(nx + 1) * P, NE = (size_t)nx * P;
   cudaStream_t st = static_cast<cudaStream_t>(s);
   Carve cv(ws);
   PcgCtl *ctl = cv.take<PcgCtl>(1);
-  double *part = cv.take<double>((size_t)sh.nb_max);
-  T *sc = cv.take<T>(sh.n_elem);
+  double *part = cv.take<double>((size_t)max_ctas(g));
+  uint8_t *mask = cv.take<uint8_t>(NN);
+  T *sc = cv.take<T>(NE);
+  T *pp = cv.take<T>(2 * NN);
+  T *app = cv.take<T>(2 * NN);
+  const dim3 fg = flat_grid(NN, 256, sm_count() * 16);
   TPO_CK(cudaMemsetAsync(ctl, 0, sizeof(PcgCtl), st));
-  k_scales_t<T><<<flat_grid(sh.n_elem, 256, 148 * 16), 256, 0, st>>>((int)sh.n_elem, rho,
-                                                                       g->e_min, g->penalty, sc);
+  if (from_density)
+    k_scales_t<T><<<flat_grid(NE, 256, sm_count() * 16), 256, 0, st>>>(nx, ny, P, elem, g->e_min,
+                                                                       g->penalty, sc);
+  else
+    k_pad_elems<T><<<flat_grid(NE, 256, sm_count() * 16), 256, 0, st>>>(nx, ny, P, elem, sc);
   TPO_CK_LAUNCH();
-  StArgs a{};
-  a.nx = g->nelx;
-  a.ny = g->nely;
+  k_pack_mask<<<fg, 256, 0, st>>>(nx, ny, P, fixed, mask);
+  TPO_CK_LAUNCH();
+  k_pack_nodes_t<T><<<fg, 256, 0, st>>>(nx, ny, P, p, pp);
+  TPO_CK_LAUNCH();
+  TsArgs a{};
+  a.nx = nx;
+  a.ny = ny;
+  a.P = P;
   a.s = sc;
-  a.fixed = fixed;
-  a.in = p;
-  a.out = ap;
+  a.mask = mask;
+  a.a = pp;
+  a.out = app;
   a.part = part;
   a.ctl = ctl;
   a.result = pap_out;
-  k_stencil<T, M_RAW, TPO_PRECOND_NONE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(a);
+  a.err = &ctl->err;
+  cudaEvent_t *ev = nullptr;
+  if (g_prof_on && (rc = prof_events(1, &ev))) return rc;
+  if (ev) TPO_CK(cudaEventRecord(ev[0], st));
+  StencilCfg<T, C, M_RAW, TPO_PRECOND_NONE>::launch(st, a, nx, ny);
   TPO_CK_LAUNCH();
-  return TPO_OK;
-}
-
-template <typename T>
-static int apply_impl(const tpo_grid *g, const T *scale, const uint8_t *fixed, const T *p, T *ap,
-                      double *pap_out, void *ws, size_t ws_bytes, tpo_stream s) {
-  int rc = check_grid(g);
-  if (rc) return rc;
-  int dev;
-  if ((rc = need_stiffness(&dev))) return rc;
-  if (!scale || !fixed || !p || !ap || !ws) return fail(TPO_ERR_ARGS, "NULL pointer argument");
-  if (!aligned(p, 2 * sizeof(T)) || !aligned(ap, 2 * sizeof(T)) || !aligned(ws, kAlign))
-    return fail(TPO_ERR_ARGS, "misaligned pointer");
-  if (ws_bytes < tpo_matvec_workspace_bytes(g))
-    return fail(TPO_ERR_WORKSPACE, "workspace too small");
-  const Shapes sh = shapes(g);
-  cudaStream_t st = static_cast<cudaStream_t>(s);
-  Carve cv(ws);
-  PcgCtl *ctl = cv.take<PcgCtl>(1);
-  double *part = cv.take<double>((size_t)sh.nb_max);
-  TPO_CK(cudaMemsetAsync(ctl, 0, sizeof(PcgCtl), st));
-  StArgs a{};
-  a.nx = g->nelx;
-  a.ny = g->nely;
-  a.s = scale;
-  a.fixed = fixed;
-  a.in = p;
-  a.out = ap;
-  a.part = part;
-  a.ctl = ctl;
-  a.result = pap_out;
-  k_stencil<T, M_RAW, TPO_PRECOND_NONE, kStripL><<<sh.st, ST_THREADS, 0, st>>>(a);
+  if (ev) {
+    TPO_CK(cudaEventRecord(ev[1], st));
+    TPO_CK(cudaEventSynchronize(ev[1]));
+    float ms = 0.f;
+    TPO_CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    const int64_t nn = (int64_t)(nx + 1) * (ny + 1);
+    g_prof.apply_launches += 1;
+    g_prof.apply_ms += ms;
+    g_prof.apply_bytes += 4 * nn * (int64_t)sizeof(T) + (int64_t)nx * ny * sizeof(T) + nn;
+  }
+  k_unpack_nodes_t<T><<<flat_grid((size_t)(nx + 1) * (ny + 1), 256, sm_count() * 16), 256, 0,
+                        st>>>(nx, ny, P, app, ap);
   TPO_CK_LAUNCH();
   return TPO_OK;
 }
@@ -623,11 +809,17 @@ int tpo_set_stiffness(const double ke[64], const double ke_inv[64], double alpha
   int dev;
   int rc = current_device(&dev);
   if (rc) return rc;
-  float kf[64], kif[64];
+  double kst[4];
+  rc = stiffness_structure(ke, kst);
+  if (rc) return rc;
+  float kf[64], kif[64], kstf[4];
   for (int i = 0; i < 64; ++i) {
     kf[i] = (float)ke[i];
     kif[i] = (float)ke_inv[i];
   }
+  for (int i = 0; i < 4; ++i) kstf[i] = (float)kst[i];
+  TPO_CK(cudaMemcpyToSymbol(c_kst, kst, sizeof(kst)));
+  TPO_CK(cudaMemcpyToSymbol(c_kst_f, kstf, sizeof(kstf)));
   TPO_CK(cudaMemcpyToSymbol(c_ke, ke, sizeof(double) * 64));
   TPO_CK(cudaMemcpyToSymbol(c_ke_f, kf, sizeof(float) * 64));
   TPO_CK(cudaMemcpyToSymbol(c_kinv, ke_inv, sizeof(double) * 64));
@@ -640,34 +832,40 @@ int tpo_set_stiffness(const double ke[64], const double ke_inv[64], double alpha
 // ------------------------------------------------------------------ matvec
 size_t tpo_matvec_workspace_bytes(const tpo_grid *g) {
   if (check_grid(g)) return 0;
-  const Shapes sh = shapes(g);
+  const int P = pad_pitch(g->nely);
+  const size_t NN = (size_t)(g->nelx + 1) * P, NE = (size_t)g->nelx * P;
   Carve cv(nullptr);
   cv.take<PcgCtl>(1);
-  cv.take<double>((size_t)sh.nb_max);
-  cv.take<double>(sh.n_elem);
+  cv.take<double>((size_t)max_ctas(g));
+  cv.take<uint8_t>(NN);
+  cv.take<double>(NE);
+  cv.take<double>(2 * NN);
+  cv.take<double>(2 * NN);
   return cv.off;
 }
 
+// The FP32 entry points compute in FP32 (the reference's precision); the FP64
+// ones in FP64.
 int tpo_matvec_f64(const tpo_grid *g, const double *rho, const uint8_t *fixed, const double *p,
                    double *ap, double *pap_out, void *ws, size_t ws_bytes, tpo_stream s) {
-  return matvec_impl<double>(g, rho, fixed, p, ap, pap_out, ws, ws_bytes, s);
+  return apply_impl<double, double>(g, rho, true, fixed, p, ap, pap_out, ws, ws_bytes, s);
 }
 
 int tpo_matvec_f32(const tpo_grid *g, const float *rho, const uint8_t *fixed, const float *p,
                    float *ap, double *pap_out, void *ws, size_t ws_bytes, tpo_stream s) {
-  return matvec_impl<float>(g, rho, fixed, p, ap, pap_out, ws, ws_bytes, s);
+  return apply_impl<float, float>(g, rho, true, fixed, p, ap, pap_out, ws, ws_bytes, s);
 }
 
 int tpo_apply_stiffness_f64(const tpo_grid *g, const double *scale, const uint8_t *fixed,
                             const double *p, double *ap, double *pap_out, void *ws,
                             size_t ws_bytes, tpo_stream s) {
-  return apply_impl<double>(g, scale, fixed, p, ap, pap_out, ws, ws_bytes, s);
+  return apply_impl<double, double>(g, scale, false, fixed, p, ap, pap_out, ws, ws_bytes, s);
 }
 
 int tpo_apply_stiffness_f32(const tpo_grid *g, const float *scale, const uint8_t *fixed,
                             const float *p, float *ap, double *pap_out, void *ws,
                             size_t ws_bytes, tpo_stream s) {
-  return apply_impl<float>(g, scale, fixed, p, ap, pap_out, ws, ws_bytes, s);
+  return apply_impl<float, float>(g, scale, false, fixed, p, ap, pap_out, ws, ws_bytes, s);
 }
 
 // ------------------------------------------------------------------ profiling
@@ -719,8 +917,8 @@ int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_p
 
   // reference solver.py:59-63: ||f|| < 1e-30 -> u = 0, no iterations
   if (std::sqrt(c->f_norm_sq) < 1e-30) {
-    const Shapes sh = shapes(g);
-    TPO_CK(cudaMemsetAsync(u, 0, 2 * sh.n_nodes * sizeof(double), st));
+    const size_t nn = (size_t)(g->nelx + 1) * (g->nely + 1);
+    TPO_CK(cudaMemsetAsync(u, 0, 2 * nn * sizeof(double), st));
     TPO_CK(cudaStreamSynchronize(st));
     out->status = TPO_SOLVE_ZERO_RHS;
     return TPO_OK;

@@ -22,6 +22,16 @@ __constant__ float c_ke_f[64];
 __constant__ double c_kinv[64];
 __constant__ float c_kinv_f[64];
 
+// Square-Q4 structure of Ke: Ke = B0^T D B0 + ch (hx hx^T + hy hy^T), where B0
+// is the strain matrix at the element centre and hx, hy the hourglass modes.
+// {k11, k12, k33, ch} = {D11/4, D12/4, D33/4, ch}, derived from the uploaded Ke
+// and checked against it entry by entry (tpo_set_stiffness).
+__constant__ double c_kst[4];
+__constant__ float c_kst_f[4];
+template <typename T> __device__ __forceinline__ T kst(int i);
+template <> __device__ __forceinline__ double kst<double>(int i) { return c_kst[i]; }
+template <> __device__ __forceinline__ float kst<float>(int i) { return c_kst_f[i]; }
+
 template <typename T, bool INV> __device__ __forceinline__ T kmat(int i);
 template <> __device__ __forceinline__ double kmat<double, false>(int i) { return c_ke[i]; }
 template <> __device__ __forceinline__ float kmat<float, false>(int i) { return c_ke_f[i]; }
@@ -78,13 +88,16 @@ struct PcgCtl {
   double rr;        // latest ||r||^2
   double pap;       // latest p.Ap
   double tol_sq;    // stop when rr < tol_sq
-  double rel_tol2;  // > 0: tol_sq = rel_tol2 * rr0 at initialisation (inner solves)
+  double rupd2;     // mixed form: replace the residual when rr < rupd2 * rmax2 (0: plain)
+  double rmax2;     // mixed form: ||r||^2 at the last FP64 residual evaluation
   int32_t it;       // completed updates
-  int32_t status;   // TPO_SOLVE_*
+  int32_t status;   // TPO_SOLVE_* (or SOLVE_NEED_UPDATE)
   int32_t max_iter;
   int32_t first;    // 1: the next direction is p = z
+  int32_t cont;     // mixed form: 1 after a residual replacement (keep p)
+  int32_t err;      // nonzero: a bounded wait ran out (TMA pipeline)
   uint32_t counter; // last-CTA ticket
-  int32_t pad;
+  int32_t since;    // mixed form: iterations since the last residual replacement
 };
 
 // Outer refinement state of the mixed-precision solve.

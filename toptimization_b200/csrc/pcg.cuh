@@ -1,188 +1,274 @@
-// PCG kernels. One CG iteration is two launches:
-//   k_stencil<DIR>   p = z + beta p (z from r on the fly, or the stored z of
+// PCG kernels on the padded layout (layout.cuh). One CG iteration is two
+// launches:
+//   k_tstencil<DIR>  p = z + beta p (z from r on the fly, or the stored z of
 //                    the element-block preconditioner), Ap = K p, p.Ap;
 //                    its last CTA sets alpha (or flags a breakdown).
 //   k_update / k_blockpre<UPDATE>
 //                    u += alpha p, r -= alpha Ap, z = M r, r.z, ||r||^2;
-//                    its last CTA tests convergence and sets beta.
+//                    its last CTA decides convergence / refinement and beta.
 // alpha, beta and the stop test never leave the device (PcgCtl). Every CTA
 // reads the status word first and returns at once when the solve is over, so
 // a host may enqueue more iterations than needed.
 //
-// Stencil kernels march along x: lane = grid row y, each thread walks a strip
-// of L node columns keeping a 3x3 window of nodal values in registers; the
-// y-neighbours come from warp shuffles. A warp computes 30 rows and uses its
-// first and last lane only as halo (warps overlap by two rows), so every lane
-// runs the same code. Strips overlap by one column on each side; values read
-// there are recomputed from their inputs, never read back from a neighbouring
-// strip's output, and the direction p ping-pongs between two buffers so that
-// no CTA overwrites what another still reads.
+// T is the storage type of the vectors and scales, C the arithmetic type:
+// <double,double> for the plain FP64 solve, <float,double> for the inner
+// solve of the mixed form (FP32 bytes, FP64 arithmetic and dots).
+//
+// k_tstencil: each CTA owns 120 grid rows (4 warps x 30; a warp's first and
+// last lane are halo rows) and walks a strip of L node columns. Column windows
+// of every input are staged into shared memory by TMA bulk copies
+// (cp.async.bulk) in groups of G columns, NG groups in flight, completion on
+// one mbarrier per ring slot; thread 0 produces, every thread consumes. Each
+// thread keeps the 3x3 neighbourhood of transformed nodal values in registers,
+// y neighbours arrive by warp shuffles. Strips overlap by two columns; values
+// there are recomputed from the inputs, never read from another strip's
+// output, and the direction p ping-pongs between two buffers so no CTA
+// overwrites what another still reads.
 #pragma once
 
 #include "common.cuh"
+#include "layout.cuh"
 #include "stencil.cuh"
 
 namespace tpo {
 
-constexpr int ST_THREADS = 128;  // 4 warps per CTA for the stencil kernels
-constexpr int ROWS_PER_WARP = 30;
+constexpr int ST_THREADS = WPC * 32;  // 128
+constexpr int UP_THREADS = 128;
 
 enum StMode { M_RAW = 0, M_DIR = 1, M_RES = 2, M_RESX = 3 };
 
-struct StArgs {
-  int nx, ny;
-  const void *s;          // element scales (T)
-  const uint8_t *fixed;   // per-node mask
-  const void *in;         // RAW: x; RES/RESX: u
+// solve status used only between the inner kernels and the host of the mixed
+// form: the FP32 residual dropped enough, an FP64 residual replacement is due
+constexpr int SOLVE_NEED_UPDATE = 6;
+constexpr int kReplaceEvery = 1000;  // mixed form: longest run between FP64 residuals
+constexpr int ERR_TMA_TIMEOUT = 1;
+
+template <typename C, typename T> __device__ __forceinline__ V2<C> cvt2(V2<T> v) {
+  return mk2<C>(C(v.x), C(v.y));
+}
+
+struct TsArgs {
+  int nx, ny, P;
+  const void *s;          // element scales (T, padded)
+  const uint8_t *mask;    // fixed mask (padded)
+  const void *a;          // RAW: x; DIR: r (point precond) or z (block); RES/RESX: u
+  void *pa, *pb;          // DIR: direction ping-pong (T)
   void *out;              // RAW: y; DIR: Ap; RES: r; RESX: inner r (float)
   void *uw;               // RES/RESX: u written back with fixed DOFs zeroed
-  const void *f;          // RES/RESX: right-hand side (T / double)
-  const void *r;          // DIR: residual (point preconditioners)
-  const void *z;          // DIR: stored z (element-block preconditioner)
-  void *pa, *pb;          // DIR: direction buffers, src/dst chosen by it parity
-  void *d;                // RESX: inner correction, zeroed
-  double *part;           // partial sums
-  PcgCtl *ctl;            // solve state (RESX: the inner solve)
-  OuterCtl *octl;         // RESX: refinement state
-  double *result;         // RAW: optional p.Ap output
+  const void *f;          // RES/RESX: right-hand side (T)
+  void *d;                // RESX: inner correction, zeroed (float)
+  double *part;
+  PcgCtl *ctl;
+  OuterCtl *octl;
+  double *result;         // RAW: optional p.Ap
+  int *err;               // TMA timeout flag
 };
 
-// ---------------------------------------------------------------------------
-// Stencil kernel: K applied to a transformed nodal field.
-// ---------------------------------------------------------------------------
-template <typename T, int MODE, int PRE, int L>
-__global__ void __launch_bounds__(ST_THREADS) k_stencil(StArgs a) {
+template <typename T, int MODE> struct TsGeom {
+  static constexpr bool HAS_B = MODE == M_DIR;
+  static constexpr int CNB = N_WIN * 2 * (int)sizeof(T);   // node bytes per column
+  static constexpr int CEB = EWin<T>::N * (int)sizeof(T);  // element bytes per column
+  static constexpr int CMB = M_WIN;                        // mask bytes per column
+  template <int G> __host__ __device__ static constexpr int slot_bytes() {
+    return G * (CNB * (HAS_B ? 2 : 1) + CEB + CMB);
+  }
+};
+
+template <typename T, typename C, int MODE, int PRE, int G, int NG>
+__global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
+  using Geo = TsGeom<T, MODE>;
   constexpr int NV = (MODE == M_RAW || MODE == M_DIR) ? 1 : (MODE == M_RES ? 2 : 3);
+  constexpr int SLOT = Geo::template slot_bytes<G>();
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[NG];   // group staged (TMA transaction bytes)
+  __shared__ __align__(8) uint64_t empty[NG];  // group consumed by all warps
+
   PcgCtl *ctl = a.ctl;
-  double beta = 0.0;
+  C beta = C(0);
   bool first = true;
   int parity = 0;
   if constexpr (MODE == M_DIR) {
     if (ctl->status != TPO_SOLVE_RUNNING) return;
-    beta = ctl->beta;
+    beta = C(ctl->beta);
     first = ctl->first != 0;
     parity = ctl->it & 1;
   }
   if constexpr (MODE == M_RESX) {
     if (a.octl->status != TPO_SOLVE_RUNNING) return;
   }
-  const int nx = a.nx, ny = a.ny;
-  const size_t ny1 = (size_t)ny + 1;
-  const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int y = gw * ROWS_PER_WARP - 1 + lane;
-  const bool row_ok = (y >= 0) && (y <= ny);
-  const bool own_row = row_ok && lane >= 1 && lane <= ROWS_PER_WARP;
+  const int nx = a.nx, ny = a.ny, P = a.P;
+  const int Y0 = blockIdx.x * RPC;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int y = Y0 + wid * RPW - 1 + lane;
+  const bool own_row = lane >= 1 && lane <= RPW && y <= ny;
   const int x0 = blockIdx.y * L;
   const int x1 = min(x0 + L, nx + 1);
-  const T *__restrict__ s = static_cast<const T *>(a.s);
+  const int cA = x0 - 2;               // first staged column
+  const int NC = x1 - cA + 1;          // staged columns cA..x1
+  const int NGRP = (NC + G - 1) / G;
+  const int ms = (Y0 + LEAD - 1) & ~15;  // first staged mask byte of a column
 
-  const T *src_p = nullptr;
-  T *dst_p = nullptr;
+  const T *gs = static_cast<const T *>(a.s);
+  const T *ga = static_cast<const T *>(a.a);
+  T *src_p = nullptr, *dst_p = nullptr;
   if constexpr (MODE == M_DIR) {
-    src_p = static_cast<const T *>(parity ? a.pb : a.pa);
+    src_p = static_cast<T *>(parity ? a.pb : a.pa);
     dst_p = static_cast<T *>(parity ? a.pa : a.pb);
   }
 
-  // element scale columns c-2, c-1, c  (rows y-1 = d, y = u)
-  T e0d = T(0), e0u = T(0), e1d = T(0), e1u = T(0), e2d, e2u;
-  load_elem_col<T>(s, x0 - 2, y, nx, ny, e2d, e2u);
-  // node columns c-2, c-1, c: values at rows y-1, y, y+1 and the mask at y
-  const V2<T> zero2 = mk2<T>(T(0), T(0));
-  V2<T> n0d = zero2, n0m = zero2, n0u = zero2, n1d = zero2, n1m = zero2, n1u = zero2;
-  V2<T> n2d = zero2, n2m = zero2, n2u = zero2;
-  unsigned m1 = 0, m2 = 0;
+  // ---- producer (thread 0): stage group g into ring slot g % NG. A slot is
+  // reused only after every warp has released the group it held (empty[]),
+  // and the producer refills with a lag of one group, so warps may drift
+  // apart by a group without waiting for each other.
+  auto issue = [&](int g) {
+    unsigned char *sb = smem + (g % NG) * SLOT;
+    unsigned bytes = 0;
+    for (int k = 0; k < G; ++k) {
+      const int c = cA + g * G + k;
+      if (c > x1) break;
+      if (c > cA && c >= 0 && c <= nx) bytes += Geo::CNB * (Geo::HAS_B ? 2 : 1) + Geo::CMB;
+      if (c >= 0 && c < nx) bytes += Geo::CEB;
+    }
+    mbar_arrive_expect_tx(&full[g % NG], bytes);
+    for (int k = 0; k < G; ++k) {
+      const int c = cA + g * G + k;
+      if (c > x1) break;
+      if (c > cA && c >= 0 && c <= nx) {
+        const size_t col = (size_t)c * P + Y0 + N_OFF;
+        bulk_g2s(sb + k * Geo::CNB, ga + 2 * col, Geo::CNB, &full[g % NG]);
+        if constexpr (Geo::HAS_B)
+          bulk_g2s(sb + G * Geo::CNB + k * Geo::CNB, src_p + 2 * col, Geo::CNB, &full[g % NG]);
+        bulk_g2s(sb + G * Geo::CNB * (Geo::HAS_B ? 2 : 1) + G * Geo::CEB + k * Geo::CMB,
+                 a.mask + (size_t)c * P + ms, Geo::CMB, &full[g % NG]);
+      }
+      if (c >= 0 && c < nx) {
+        bulk_g2s(sb + G * Geo::CNB * (Geo::HAS_B ? 2 : 1) + k * Geo::CEB,
+                 gs + (size_t)c * P + Y0 + EWin<T>::OFF, Geo::CEB, &full[g % NG]);
+      }
+    }
+  };
+  bool ok = true;
+  // refill slot g % NG with group g once its previous tenant (g - NG) is released
+  auto refill = [&](int g) {
+    if (g >= NGRP) return;
+    if (g >= NG && ok)
+      ok = mbar_wait_bounded(&empty[g % NG], ((g / NG) - 1) & 1, a.err, ERR_TMA_TIMEOUT);
+    issue(g);
+  };
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NG; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], WPC);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int g = 0; g < NG - 1 && g < NGRP; ++g) issue(g);
+  }
+
+  // per-lane indices inside the staged column windows
+  const int n_idx = y - Y0 + 2;
+  const int e_idx = y - Y0 + (LEAD - 1 - EWin<T>::OFF);  // element row y-1; row y is +1
+  const int m_idx = y + LEAD - ms;
+
+  // Element-centric march. At step c lane y transforms node (c, y) (p_new,
+  // or u with fixed DOFs zeroed), forms element (c-1, y) from its corners
+  // (c-1, y) (c, y) (c, y+1) (c-1, y+1), and finishes node (c-1, y): the carry
+  // holds what elements (c-2, y) and (c-2, y-1) gave it one step earlier.
+  const V2<C> zero2 = mk2<C>(C(0), C(0));
+  V2<C> pn_prev = zero2, pu_prev = zero2, carry = zero2;
+  C sprev_d = C(0), sprev_u = C(0);  // element column c-1, rows y-1, y
+  C s2_d = C(0), s2_u = C(0);        // element column c-2, rows y-1, y (residual modes)
+  unsigned m_prev = 0;
   double acc[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
 
-  // Raw inputs of one column, fetched one column ahead so that its loads are
-  // in flight while the current column is computed.
-  struct Raw {
-    T sd, su;
-    V2<T> a, b;
-    unsigned m;
-  };
-  auto fetch = [&](int c, Raw &R) {
-    load_elem_col<T>(s, c, y, nx, ny, R.sd, R.su);
-    R.m = 0;
-    R.a = zero2;
-    R.b = zero2;
-    if (row_ok && c >= 0 && c <= nx) {
-      const size_t node = (size_t)c * ny1 + y;
-      R.m = a.fixed[node];
-      if constexpr (MODE == M_DIR) {
-        if constexpr (PRE == TPO_PRECOND_BLOCK_JACOBI) R.a = ld2<T>(static_cast<const T *>(a.z), node);
-        else R.a = ld2<T>(static_cast<const T *>(a.r), node);
-        if (!first) R.b = ld2<T>(src_p, node);
-      } else {
-        R.a = ld2<T>(static_cast<const T *>(a.in), node);
-      }
-    }
-  };
-  Raw nxt;
-  fetch(x0 - 1, nxt);
-
-  for (int c = x0 - 1; c <= x1; ++c) {
-    const Raw cur = nxt;
-    if (c < x1) fetch(c + 1, nxt);
-    e0d = e1d; e0u = e1u; e1d = e2d; e1u = e2u;
-    e2d = cur.sd;
-    e2u = cur.su;
+  for (int k = 0; k < NC; ++k) {
+    const int c = cA + k;
+    const int g = k / G, kk = k - g * G;
+    if (kk == 0 && ok) ok = mbar_wait_bounded(&full[g % NG], (g / NG) & 1, a.err, ERR_TMA_TIMEOUT);
+    const unsigned char *sb = smem + (g % NG) * SLOT;
+    const V2<T> *colA = reinterpret_cast<const V2<T> *>(sb + kk * Geo::CNB);
+    const V2<T> *colB = reinterpret_cast<const V2<T> *>(sb + G * Geo::CNB + kk * Geo::CNB);
+    const T *colS = reinterpret_cast<const T *>(sb + G * Geo::CNB * (Geo::HAS_B ? 2 : 1) +
+                                                kk * Geo::CEB);
+    const uint8_t *colM = sb + G * Geo::CNB * (Geo::HAS_B ? 2 : 1) + G * Geo::CEB + kk * Geo::CMB;
+    const bool node_ok = c > cA && c >= 0 && c <= nx;  // column cA stages scales only
+    const bool elem_ok = c >= 0 && c < nx;
+    const C scd = elem_ok ? C(colS[e_idx]) : C(0);      // element (c, y-1)
+    const C scu = elem_ok ? C(colS[e_idx + 1]) : C(0);  // element (c, y)
 
     // ---- transformed nodal value at (c, y)
-    V2<T> v = zero2;
-    const unsigned m = cur.m;
-    if (row_ok && c >= 0 && c <= nx) {
+    V2<C> v = zero2;
+    const unsigned m = node_ok ? colM[m_idx] : 0u;
+    if (node_ok) {
+      const V2<C> av = cvt2<C, T>(colA[n_idx]);
       if constexpr (MODE == M_RAW) {
-        v = cur.a;
+        v = av;
       } else if constexpr (MODE == M_DIR) {
-        V2<T> z;
-        if constexpr (PRE == TPO_PRECOND_BLOCK_JACOBI) z = cur.a;
-        else z = point_precond<T, PRE>(cur.a, m, e1d, e1u, e2d, e2u);
-        if (first) v = z;
-        else v = mk2<T>(fmaT(T(beta), cur.b.x, z.x), fmaT(T(beta), cur.b.y, z.y));
+        V2<C> z;
+        if constexpr (PRE == TPO_PRECOND_BLOCK_JACOBI) z = av;
+        else z = point_precond<C, PRE>(av, m, sprev_d, sprev_u, scd, scu);
+        if (first) {
+          v = z;
+        } else {
+          const V2<C> po = cvt2<C, T>(colB[n_idx]);
+          v = mk2<C>(fmaT(beta, po.x, z.x), fmaT(beta, po.y, z.y));
+        }
+        v = cvt2<C, T>(mk2<T>(T(v.x), T(v.y)));  // the stored direction is what K sees
       } else {  // M_RES, M_RESX: u with fixed DOFs zeroed (idempotent write-back)
-        v = cur.a;
-        if (m & FIXED_X) v.x = T(0);
-        if (m & FIXED_Y) v.y = T(0);
+        v = av;
+        if (m & FIXED_X) v.x = C(0);
+        if (m & FIXED_Y) v.y = C(0);
         if (m && own_row && c >= x0 && c < x1)
-          st2<T>(static_cast<T *>(a.uw), (size_t)c * ny1 + y, v);
+          st2<T>(static_cast<T *>(a.uw), pslot(c, y, P), mk2<T>(T(v.x), T(v.y)));
       }
     }
-    n0d = n1d; n0m = n1m; n0u = n1u;
-    n1d = n2d; n1m = n2m; n1u = n2u;
-    m1 = m2;
-    m2 = m;
-    n2m = v;
-    n2d = shfl_up2<T>(v);
-    n2u = shfl_down2<T>(v);
+    const V2<C> vu = shfl_down2<C>(v);  // node (c, y+1)
 
-    // ---- output at node (xo, y), xo = c - 1
+    // ---- element (c-1, y): corners (c-1,y) (c,y) (c,y+1) (c-1,y+1)
+    V2<C> fbl, fbr, ftr, ftl;
+    elem_forces<C>(sprev_u, pn_prev, v, vu, pu_prev, fbl, fbr, ftr, ftl);
+    const V2<C> tl_below = shfl_up2<C>(ftl);  // element (c-1, y-1) -> node (c-1, y)
+    const V2<C> tr_below = shfl_up2<C>(ftr);  // element (c-1, y-1) -> node (c, y)
+
+    // this warp is done with group g: release it; thread 0 then stages
+    // group g + NG - 1 into the slot of group g - 1
+    if (kk == G - 1 || k == NC - 1) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[g % NG]);
+      if (threadIdx.x == 0) refill(g + NG - 1);
+    }
+
+    // ---- node (xo, y), xo = c - 1, is complete
     const int xo = c - 1;
     if (own_row && xo >= x0) {
-      const size_t node = (size_t)xo * ny1 + y;
-      V2<T> kv = node_apply<T, false>(n0d, n0m, n0u, n1d, n1m, n1u, n2d, n2m, n2u, e0d, e0u,
-                                      e1d, e1u);
-      if (m1 & FIXED_X) kv.x = n1m.x;  // identity rows at fixed DOFs
-      if (m1 & FIXED_Y) kv.y = n1m.y;
+      const size_t node = pslot(xo, y, P);
+      V2<C> kv = mk2<C>(carry.x + fbl.x + tl_below.x, carry.y + fbl.y + tl_below.y);
+      if (m_prev & FIXED_X) kv.x = pn_prev.x;  // identity rows at fixed DOFs
+      if (m_prev & FIXED_Y) kv.y = pn_prev.y;
       if constexpr (MODE == M_RAW) {
-        st2<T>(static_cast<T *>(a.out), node, kv);
-        acc[0] += (double)n1m.x * kv.x + (double)n1m.y * kv.y;
+        const V2<T> ks = mk2<T>(T(kv.x), T(kv.y));
+        st2<T>(static_cast<T *>(a.out), node, ks);
+        acc[0] += (double)pn_prev.x * (double)ks.x + (double)pn_prev.y * (double)ks.y;
       } else if constexpr (MODE == M_DIR) {
-        st2<T>(dst_p, node, n1m);
-        st2<T>(static_cast<T *>(a.out), node, kv);
-        acc[0] += (double)n1m.x * kv.x + (double)n1m.y * kv.y;
+        const V2<T> ks = mk2<T>(T(kv.x), T(kv.y));
+        st2<T>(dst_p, node, mk2<T>(T(pn_prev.x), T(pn_prev.y)));
+        st2<T>(static_cast<T *>(a.out), node, ks);
+        acc[0] += (double)pn_prev.x * (double)ks.x + (double)pn_prev.y * (double)ks.y;
       } else if constexpr (MODE == M_RES) {
-        const V2<T> f = ld2<T>(static_cast<const T *>(a.f), node);
-        const V2<T> r = mk2<T>(f.x - kv.x, f.y - kv.y);
+        const V2<C> f = cvt2<C, T>(ld2<T>(static_cast<const T *>(a.f), node));
+        const V2<T> r = mk2<T>(T(f.x - kv.x), T(f.y - kv.y));
         st2<T>(static_cast<T *>(a.out), node, r);
         if constexpr (PRE != TPO_PRECOND_BLOCK_JACOBI) {
-          const V2<T> z = point_precond<T, PRE>(r, m1, e0d, e0u, e1d, e1u);
+          const V2<C> z = point_precond<C, PRE>(cvt2<C, T>(r), m_prev, s2_d, s2_u, sprev_d,
+                                                sprev_u);
           acc[0] += (double)r.x * z.x + (double)r.y * z.y;
         }
         acc[1] += (double)r.x * r.x + (double)r.y * r.y;
-      } else {  // M_RESX: T == double; inner solve in float
+      } else {  // M_RESX: T == C == double; the inner solve stores float
         const double2 f = ld2<double>(static_cast<const double *>(a.f), node);
         const double rx = f.x - (double)kv.x, ry = f.y - (double)kv.y;
         acc[0] += rx * rx + ry * ry;
@@ -190,15 +276,32 @@ __global__ void __launch_bounds__(ST_THREADS) k_stencil(StArgs a) {
         st2<float>(static_cast<float *>(a.out), node, r32);
         st2<float>(static_cast<float *>(a.d), node, make_float2(0.f, 0.f));
         if constexpr (PRE != TPO_PRECOND_BLOCK_JACOBI) {
-          const float2 z = point_precond<float, PRE>(r32, m1, (float)e0d, (float)e0u,
-                                                     (float)e1d, (float)e1u);
+          // the inner kernels see FP32-stored scales: use the same here
+          const double2 z = point_precond<double, PRE>(
+              make_double2(r32.x, r32.y), m_prev, (double)(float)s2_d, (double)(float)s2_u,
+              (double)(float)sprev_d, (double)(float)sprev_u);
           acc[1] += (double)r32.x * z.x + (double)r32.y * z.y;
         }
         acc[2] += (double)r32.x * r32.x + (double)r32.y * r32.y;
       }
     }
+    carry = mk2<C>(fbr.x + tr_below.x, fbr.y + tr_below.y);
+    pn_prev = v;
+    pu_prev = vu;
+    s2_d = sprev_d;
+    s2_u = sprev_u;
+    sprev_d = scd;
+    sprev_u = scu;
+    m_prev = m;
   }
 
+  if (!ok) {
+    // a wait ran out: drain this CTA's copies (bounded) before its shared
+    // memory is released; the result is discarded by the host (err flag)
+    for (int g = (NGRP > NG ? NGRP - NG : 0); g < NGRP; ++g)
+      mbar_wait_bounded(&full[g % NG], (g / NG) & 1, nullptr, 0);
+  }
+  __syncthreads();  // no warp leaves while thread 0 may still be staging
   uint32_t *counter = (MODE == M_RESX) ? &a.octl->counter : &ctl->counter;
   if (!grid_reduce<NV>(acc, a.part, counter)) return;
   if (threadIdx.x != 0) return;
@@ -218,35 +321,41 @@ __global__ void __launch_bounds__(ST_THREADS) k_stencil(StArgs a) {
     if (PRE != TPO_PRECOND_BLOCK_JACOBI) ctl->rz = acc[0];
     if (!finite(acc[0]) || !finite(acc[1])) ctl->status = TPO_SOLVE_NONFINITE;
   } else {
+    // FP64 residual of the mixed form: first residual of the solve, or a
+    // replacement of the inner recursive residual ("reliable update")
     OuterCtl *o = a.octl;
     o->rr = acc[0];
     o->it += 1;
-    if (!finite(acc[0])) {
-      o->status = TPO_SOLVE_NONFINITE;
-    } else if (acc[0] < o->tol_sq) {
-      o->status = TPO_SOLVE_CONVERGED;
-    }
-    // (re)initialise the inner solve on this residual
-    ctl->it = 0;
-    ctl->first = 1;
+    const bool cont = o->it > 1;
+    if (!finite(acc[0]) || !finite(acc[1]) || !finite(acc[2])) o->status = TPO_SOLVE_NONFINITE;
+    else if (acc[0] < o->tol_sq) o->status = TPO_SOLVE_CONVERGED;
+    ctl->rmax2 = acc[0];
+    ctl->since = 0;
     ctl->rr = acc[2];
+    ctl->cont = cont ? 1 : 0;
     if (PRE != TPO_PRECOND_BLOCK_JACOBI) {
+      if (cont) {
+        ctl->beta = acc[1] / (ctl->rz + 1e-60);  // keep the direction
+        ctl->first = 0;
+      } else {
+        ctl->first = 1;
+      }
       ctl->rz = acc[1];
-      ctl->tol_sq = ctl->rel_tol2 * acc[2];
     }
     ctl->status = (o->status == TPO_SOLVE_RUNNING) ? TPO_SOLVE_RUNNING : TPO_SOLVE_CONVERGED;
   }
 }
 
 // ---------------------------------------------------------------------------
-// Point-preconditioner update: u += alpha p, r -= alpha Ap, z = M r (z not
-// stored: the next direction kernel recomputes it), r.z and ||r||^2.
-// Pointwise, so a warp covers 32 rows with no halo.
+// Point-preconditioner update (pointwise; a warp covers 32 rows, no halo):
+// u += alpha p, r -= alpha Ap, z = M r (z not stored), r.z and ||r||^2.
+// Columns are processed in batches of UB: a batch's loads are issued before
+// its arithmetic.
 // ---------------------------------------------------------------------------
 struct UpdArgs {
-  int nx, ny;
+  int nx, ny, P;
   const void *s;
-  const uint8_t *fixed;
+  const uint8_t *mask;
   void *u, *r;
   const void *ap;
   const void *pa, *pb;
@@ -255,30 +364,42 @@ struct UpdArgs {
 };
 
 __device__ __forceinline__ void finish_update(PcgCtl *ctl, double rz_new, double rr) {
-  // reference solver.py:119-155: convergence on the recursive residual
-  // before the direction update; beta = rz_new / (rz_old + 1e-60)
   ctl->it += 1;
   ctl->rr = rr;
   if (!finite(rz_new) || !finite(rr)) {
     ctl->status = TPO_SOLVE_NONFINITE;
-  } else if (rr < ctl->tol_sq) {
-    ctl->status = TPO_SOLVE_CONVERGED;
-  } else if (ctl->it >= ctl->max_iter) {
-    ctl->status = TPO_SOLVE_MAX_ITER;
-  } else {
-    ctl->beta = rz_new / (ctl->rz + 1e-60);
-    ctl->rz = rz_new;
+    return;
   }
+  if (ctl->rupd2 > 0.0) {
+    // mixed form: the recursive FP32 residual only schedules an FP64
+    // residual replacement (when it has dropped by inner_tol below the
+    // largest residual seen since the last replacement, or every
+    // kReplaceEvery iterations); convergence is decided on the FP64 residual
+    ctl->rmax2 = fmax(ctl->rmax2, rr);
+    ctl->since += 1;
+    if (rr < ctl->rupd2 * ctl->rmax2 || rr < ctl->tol_sq || ctl->since >= kReplaceEvery) {
+      ctl->status = SOLVE_NEED_UPDATE;
+      return;
+    }
+  } else if (rr < ctl->tol_sq) {  // reference solver.py:147-149
+    ctl->status = TPO_SOLVE_CONVERGED;
+    return;
+  }
+  if (ctl->it >= ctl->max_iter) {
+    ctl->status = TPO_SOLVE_MAX_ITER;
+    return;
+  }
+  ctl->beta = rz_new / (ctl->rz + 1e-60);  // solver.py:151
+  ctl->rz = rz_new;
 }
 
-template <typename T, int PRE, int L>
-__global__ void __launch_bounds__(ST_THREADS) k_update(UpdArgs a) {
+template <typename T, typename C, int PRE>
+__global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
   PcgCtl *ctl = a.ctl;
   if (ctl->status != TPO_SOLVE_RUNNING) return;
-  const T alpha = T(ctl->alpha);
+  const C alpha = C(ctl->alpha);
   const T *__restrict__ p = static_cast<const T *>((ctl->it & 1) ? a.pa : a.pb);
-  const int nx = a.nx, ny = a.ny;
-  const size_t ny1 = (size_t)ny + 1;
+  const int nx = a.nx, ny = a.ny, P = a.P;
   const int y = blockIdx.x * blockDim.x + threadIdx.x;
   const bool row_ok = y <= ny;
   const int x0 = blockIdx.y * L;
@@ -288,26 +409,33 @@ __global__ void __launch_bounds__(ST_THREADS) k_update(UpdArgs a) {
   T *__restrict__ r = static_cast<T *>(a.r);
   const T *__restrict__ ap = static_cast<const T *>(a.ap);
 
-  // Columns are processed in batches of UB: all loads of a batch are issued
-  // before any of its arithmetic, so UB columns of loads are in flight.
   constexpr int UB = 4;
-  T ebd = T(0), ebu = T(0);
-  if (PRE != TPO_PRECOND_NONE) load_elem_col<T>(s, x0 - 1, y, nx, ny, ebd, ebu);
+  // element scales of column c at rows y-1, y (padded: zero outside the grid)
+  auto ld_s = [&](int c, C &sd, C &su) {
+    sd = su = C(0);
+    if (PRE != TPO_PRECOND_NONE && row_ok && c >= 0 && c < nx) {
+      const size_t e = pslot(c, y, P);
+      sd = C(s[e - 1]);
+      su = C(s[e]);
+    }
+  };
+  C ebd, ebu;
+  ld_s(x0 - 1, ebd, ebu);
   double acc[2] = {0.0, 0.0};
   for (int cb = x0; cb < x1; cb += UB) {
     V2<T> uv[UB], rv[UB], pv[UB], av[UB];
-    T sd[UB], su[UB];
+    C sd[UB], su[UB];
     unsigned m[UB];
 #pragma unroll
     for (int k = 0; k < UB; ++k) {
       const int c = cb + k;
-      sd[k] = su[k] = T(0);
+      sd[k] = su[k] = C(0);
       m[k] = 0;
       if (c < x1) {
-        if (PRE != TPO_PRECOND_NONE) load_elem_col<T>(s, c, y, nx, ny, sd[k], su[k]);
+        ld_s(c, sd[k], su[k]);
         if (row_ok) {
-          const size_t node = (size_t)c * ny1 + y;
-          m[k] = a.fixed[node];
+          const size_t node = pslot(c, y, P);
+          m[k] = a.mask[node];
           uv[k] = ld2<T>(u, node);
           rv[k] = ld2<T>(r, node);
           pv[k] = ld2<T>(p, node);
@@ -318,20 +446,21 @@ __global__ void __launch_bounds__(ST_THREADS) k_update(UpdArgs a) {
 #pragma unroll
     for (int k = 0; k < UB; ++k) {
       const int c = cb + k;
-      const T ead = ebd, eau = ebu;
+      const C ead = ebd, eau = ebu;
       ebd = sd[k];
       ebu = su[k];
       if (c < x1 && row_ok) {
-        const size_t node = (size_t)c * ny1 + y;
-        uv[k].x = fmaT(alpha, pv[k].x, uv[k].x);
-        uv[k].y = fmaT(alpha, pv[k].y, uv[k].y);
-        rv[k].x = fmaT(-alpha, av[k].x, rv[k].x);
-        rv[k].y = fmaT(-alpha, av[k].y, rv[k].y);
-        st2<T>(u, node, uv[k]);
-        st2<T>(r, node, rv[k]);
-        const V2<T> z = point_precond<T, PRE>(rv[k], m[k], ead, eau, ebd, ebu);
-        acc[0] += (double)rv[k].x * z.x + (double)rv[k].y * z.y;
-        acc[1] += (double)rv[k].x * rv[k].x + (double)rv[k].y * rv[k].y;
+        const size_t node = pslot(c, y, P);
+        const V2<T> un = mk2<T>(T(fmaT(alpha, C(pv[k].x), C(uv[k].x))),
+                                T(fmaT(alpha, C(pv[k].y), C(uv[k].y))));
+        const V2<T> rn = mk2<T>(T(fmaT(-alpha, C(av[k].x), C(rv[k].x))),
+                                T(fmaT(-alpha, C(av[k].y), C(rv[k].y))));
+        st2<T>(u, node, un);
+        st2<T>(r, node, rn);
+        const V2<C> rc = cvt2<C, T>(rn);
+        const V2<C> z = point_precond<C, PRE>(rc, m[k], ead, eau, ebd, ebu);
+        acc[0] += (double)rc.x * z.x + (double)rc.y * z.y;
+        acc[1] += (double)rc.x * rc.x + (double)rc.y * rc.y;
       }
     }
   }
@@ -347,37 +476,36 @@ __global__ void __launch_bounds__(ST_THREADS) k_update(UpdArgs a) {
 // UPDATE: r_new = r - alpha Ap is formed for the strip and its halo (read from
 // one residual buffer, written to the other), u += alpha p on owned nodes,
 // then z from r_new, and the convergence/beta logic.
-// INIT:   z from r as it is (first residual of a solve).
+// INIT:   z from r as it is (first residual of a solve, or a replaced one).
 // ---------------------------------------------------------------------------
 struct BlkArgs {
-  int nx, ny;
-  const void *w;        // element weights w_e (T)
-  const uint8_t *fixed;
+  int nx, ny, P;
+  const void *w;
+  const uint8_t *mask;
   void *u;
   const void *ap;
-  const void *pa, *pb;  // directions (the one the current iteration wrote)
-  void *ra, *rb;        // residual ping-pong
+  const void *pa, *pb;
+  void *ra, *rb;
   void *z;
   double *part;
   PcgCtl *ctl;
 };
 
-template <typename T, bool INIT, int L>
+template <typename T, typename C, bool INIT, int L>
 __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
   PcgCtl *ctl = a.ctl;
   if (ctl->status != TPO_SOLVE_RUNNING) return;
   const int parity = ctl->it & 1;
-  const T alpha = INIT ? T(0) : T(ctl->alpha);
-  const T *r_src = static_cast<const T *>(INIT ? a.ra : (parity ? a.rb : a.ra));
+  const C alpha = INIT ? C(0) : C(ctl->alpha);
+  const T *r_src = static_cast<const T *>(parity ? a.rb : a.ra);
   T *r_dst = static_cast<T *>(parity ? a.ra : a.rb);
   const T *__restrict__ p = static_cast<const T *>(parity ? a.pa : a.pb);
-  const int nx = a.nx, ny = a.ny;
-  const size_t ny1 = (size_t)ny + 1;
+  const int nx = a.nx, ny = a.ny, P = a.P;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int y = gw * ROWS_PER_WARP - 1 + lane;
+  const int y = gw * RPW - 1 + lane;
   const bool row_ok = (y >= 0) && (y <= ny);
-  const bool own_row = row_ok && lane >= 1 && lane <= ROWS_PER_WARP;
+  const bool own_row = row_ok && lane >= 1 && lane <= RPW;
   const int x0 = blockIdx.y * L;
   const int x1 = min(x0 + L, nx + 1);
   const T *__restrict__ w = static_cast<const T *>(a.w);
@@ -385,27 +513,33 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
   const T *__restrict__ ap = static_cast<const T *>(a.ap);
   T *__restrict__ z = static_cast<T *>(a.z);
 
-  T e0d = T(0), e0u = T(0), e1d = T(0), e1u = T(0);
-  const V2<T> zero2 = mk2<T>(T(0), T(0));
-  V2<T> n0d = zero2, n0m = zero2, n0u = zero2, n1d = zero2, n1m = zero2, n1u = zero2;
-  V2<T> n2d = zero2, n2m = zero2, n2u = zero2;
-  V2<T> rn1 = zero2, rn2 = zero2;  // unscaled residual at columns c-1, c
+  C e0d = C(0), e0u = C(0), e1d = C(0), e1u = C(0);
+  const V2<C> zero2 = mk2<C>(C(0), C(0));
+  V2<C> n0d = zero2, n0m = zero2, n0u = zero2, n1d = zero2, n1m = zero2, n1u = zero2;
+  V2<C> n2d = zero2, n2m = zero2, n2u = zero2;
+  V2<C> rn1 = zero2, rn2 = zero2;  // unscaled residual at columns c-1, c
   unsigned m1 = 0, m2 = 0;
   double acc[2] = {0.0, 0.0};
 
-  // raw inputs of column c, fetched one column ahead
   struct Raw {
-    T wd, wu;
+    C wd, wu;
     V2<T> r, ap, u, p;
     unsigned m;
   };
+  const V2<T> tz = mk2<T>(T(0), T(0));
   auto fetch = [&](int c, Raw &R) {
-    load_elem_col<T>(w, c - 1, y, nx, ny, R.wd, R.wu);
+    R.wd = R.wu = C(0);
+    const int ce = c - 1;
+    if (ce >= 0 && ce < nx && row_ok) {
+      const size_t e = pslot(ce, y, P);
+      R.wd = C(w[e - 1]);
+      R.wu = C(w[e]);
+    }
     R.m = 0;
-    R.r = R.ap = R.u = R.p = zero2;
+    R.r = R.ap = R.u = R.p = tz;
     if (row_ok && c >= 0 && c <= nx) {
-      const size_t node = (size_t)c * ny1 + y;
-      R.m = a.fixed[node];
+      const size_t node = pslot(c, y, P);
+      R.m = a.mask[node];
       R.r = ld2<T>(r_src, node);
       if (!INIT) {
         R.ap = ld2<T>(ap, node);
@@ -424,52 +558,57 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
     e0d = e1d; e0u = e1u;
     e1d = cur.wd;
     e1u = cur.wu;
-    V2<T> rt = zero2, rn = zero2;
+    V2<C> rt = zero2, rn = zero2;
     const unsigned m = cur.m;
     if (row_ok && c >= 0 && c <= nx) {
-      const size_t node = (size_t)c * ny1 + y;
-      rn = cur.r;
+      const size_t node = pslot(c, y, P);
+      rn = cvt2<C, T>(cur.r);
       if (!INIT) {
-        rn.x = fmaT(-alpha, cur.ap.x, rn.x);
-        rn.y = fmaT(-alpha, cur.ap.y, rn.y);
+        const V2<T> rs = mk2<T>(T(fmaT(-alpha, C(cur.ap.x), rn.x)),
+                                T(fmaT(-alpha, C(cur.ap.y), rn.y)));
+        rn = cvt2<C, T>(rs);
         if (own_row && c >= x0 && c < x1) {
-          V2<T> uv = cur.u;
-          uv.x = fmaT(alpha, cur.p.x, uv.x);
-          uv.y = fmaT(alpha, cur.p.y, uv.y);
-          st2<T>(u, node, uv);
-          st2<T>(r_dst, node, rn);
+          st2<T>(u, node, mk2<T>(T(fmaT(alpha, C(cur.p.x), C(cur.u.x))),
+                                 T(fmaT(alpha, C(cur.p.y), C(cur.u.y)))));
+          st2<T>(r_dst, node, rs);
         }
       }
-      const T sq = sqrt(T(node_elem_count(c, y, nx, ny)));
-      rt = mk2<T>(rn.x / sq, rn.y / sq);
+      const C sq = sqrt(C(node_elem_count(c, y, nx, ny)));
+      rt = mk2<C>(rn.x / sq, rn.y / sq);
     }
     n0d = n1d; n0m = n1m; n0u = n1u;
     n1d = n2d; n1m = n2m; n1u = n2u;
     rn1 = rn2; rn2 = rn;
     m1 = m2; m2 = m;
     n2m = rt;
-    n2d = shfl_up2<T>(rt);
-    n2u = shfl_down2<T>(rt);
+    n2d = shfl_up2<C>(rt);
+    n2u = shfl_down2<C>(rt);
 
     const int xo = c - 1;
     if (own_row && xo >= x0) {
-      const size_t node = (size_t)xo * ny1 + y;
-      V2<T> zz = node_apply<T, true>(n0d, n0m, n0u, n1d, n1m, n1u, n2d, n2m, n2u, e0d, e0u, e1d,
+      const size_t node = pslot(xo, y, P);
+      V2<C> zz = node_apply<C, true>(n0d, n0m, n0u, n1d, n1m, n1u, n2d, n2m, n2u, e0d, e0u, e1d,
                                      e1u);
-      const T sq = sqrt(T(node_elem_count(xo, y, nx, ny)));
-      zz.x = (m1 & FIXED_X) ? T(0) : zz.x / sq;
-      zz.y = (m1 & FIXED_Y) ? T(0) : zz.y / sq;
-      st2<T>(z, node, zz);
-      acc[0] += (double)rn1.x * zz.x + (double)rn1.y * zz.y;
+      const C sq = sqrt(C(node_elem_count(xo, y, nx, ny)));
+      const V2<T> zs = mk2<T>((m1 & FIXED_X) ? T(0) : T(zz.x / sq),
+                              (m1 & FIXED_Y) ? T(0) : T(zz.y / sq));
+      st2<T>(z, node, zs);
+      acc[0] += (double)rn1.x * (double)zs.x + (double)rn1.y * (double)zs.y;
       acc[1] += (double)rn1.x * rn1.x + (double)rn1.y * rn1.y;
     }
   }
   if (!grid_reduce<2>(acc, a.part, &ctl->counter)) return;
   if (threadIdx.x != 0) return;
   if (INIT) {
+    // first residual of a solve, or (mixed form) a replaced residual
+    if (ctl->cont) {
+      ctl->beta = acc[0] / (ctl->rz + 1e-60);
+      ctl->first = 0;
+    } else {
+      ctl->first = 1;
+    }
     ctl->rz = acc[0];
     ctl->rr = acc[1];
-    if (ctl->rel_tol2 > 0.0) ctl->tol_sq = ctl->rel_tol2 * acc[1];
     if (!finite(acc[0]) || !finite(acc[1])) ctl->status = TPO_SOLVE_NONFINITE;
   } else {
     finish_update(ctl, acc[0], acc[1]);
@@ -477,35 +616,58 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Per-solve setup and small helpers
+// Per-solve setup and small helpers (padded layout)
 // ---------------------------------------------------------------------------
 // s = e_min + rho^p (1 - e_min) (reference fem/kernels.py:92), its FP32 copy,
 // and the element-block weights w = s / max(s, alpha)^2 (preconditioner.py:55-57).
-__global__ void k_scales(int n, const double *__restrict__ rho, double e_min, double pen,
-                         double alpha_reg, double *__restrict__ s64, float *__restrict__ s32,
-                         double *__restrict__ w64, float *__restrict__ w32) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-    const double s = e_min + pow(rho[e], pen) * (1.0 - e_min);
-    if (s64) s64[e] = s;
-    if (s32) s32[e] = (float)s;
-    if (w64 || w32) {
+// Writes every slot of the padded arrays (pads = 0).
+__global__ void k_scales(int nx, int ny, int P, const double *__restrict__ rho, double e_min,
+                         double pen, double alpha_reg, double *__restrict__ s64,
+                         float *__restrict__ s32, double *__restrict__ w64,
+                         float *__restrict__ w32) {
+  const size_t total = (size_t)nx * P;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int ex = (int)(i / P), ey = (int)(i % P) - LEAD;
+    double s = 0.0, w = 0.0;
+    if (ey >= 0 && ey < ny) {
+      s = e_min + pow(rho[(size_t)ex * ny + ey], pen) * (1.0 - e_min);
       const double sc = fmax(s, alpha_reg);
-      const double w = s / (sc * sc);
-      if (w64) w64[e] = w;
-      if (w32) w32[e] = (float)w;
+      w = s / (sc * sc);
     }
+    if (s64) s64[i] = s;
+    if (s32) s32[i] = (float)s;
+    if (w64) w64[i] = w;
+    if (w32) w32[i] = (float)w;
   }
 }
 
+// element values (compact, T) -> SIMP scales, padded T
 template <typename T>
-__global__ void k_scales_t(int n, const T *__restrict__ rho, double e_min, double pen,
-                           T *__restrict__ s) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-    s[e] = T(e_min + pow((double)rho[e], pen) * (1.0 - e_min));
+__global__ void k_scales_t(int nx, int ny, int P, const T *__restrict__ rho, double e_min,
+                           double pen, T *__restrict__ s) {
+  const size_t total = (size_t)nx * P;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int ex = (int)(i / P), ey = (int)(i % P) - LEAD;
+    s[i] = (ey >= 0 && ey < ny)
+               ? T(e_min + pow((double)rho[(size_t)ex * ny + ey], pen) * (1.0 - e_min))
+               : T(0);
   }
 }
 
-__global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rel_tol2, int max_iter,
+// precomputed compact scales -> padded
+template <typename T>
+__global__ void k_pad_elems(int nx, int ny, int P, const T *__restrict__ src, T *__restrict__ dst) {
+  const size_t total = (size_t)nx * P;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int ex = (int)(i / P), ey = (int)(i % P) - LEAD;
+    dst[i] = (ey >= 0 && ey < ny) ? src[(size_t)ex * ny + ey] : T(0);
+  }
+}
+
+__global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rupd2, int max_iter,
                            OuterCtl *octl, double outer_tol_sq) {
   ctl->rz = 0.0;
   ctl->alpha = 0.0;
@@ -513,11 +675,15 @@ __global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rel_tol2, int max_
   ctl->rr = 0.0;
   ctl->pap = 0.0;
   ctl->tol_sq = tol_sq;
-  ctl->rel_tol2 = rel_tol2;
+  ctl->rupd2 = rupd2;
+  ctl->rmax2 = 0.0;
   ctl->it = 0;
   ctl->status = TPO_SOLVE_RUNNING;
   ctl->max_iter = max_iter;
   ctl->first = 1;
+  ctl->cont = 0;
+  ctl->since = 0;
+  ctl->err = 0;
   ctl->counter = 0u;
   if (octl) {
     octl->rr = 0.0;
@@ -528,12 +694,11 @@ __global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rel_tol2, int max_
   }
 }
 
-// Mixed precision: u += d (FP32 correction) on every DOF.
-__global__ void k_correct(size_t n2, double *__restrict__ u, const float *__restrict__ d) {
+// mixed form: u += y (FP32 correction accumulated since the last replacement)
+__global__ void k_accumulate(size_t n2, double *__restrict__ u, const float *__restrict__ y) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2;
-       i += (size_t)gridDim.x * blockDim.x) {
-    u[i] += (double)d[i];
-  }
+       i += (size_t)gridDim.x * blockDim.x)
+    u[i] += (double)y[i];
 }
 
 }  // namespace tpo

@@ -47,6 +47,29 @@ __device__ __forceinline__ V2<T> node_apply(V2<T> LD, V2<T> LM, V2<T> LU, V2<T> 
   return acc;
 }
 
+// s * Ke * p_e for one element from its corner values (BL, BR, TR, TL), using
+// Ke = B0^T D B0 + ch (hx hx^T + hy hy^T): the centre strain (ex, ey, g) and
+// the two hourglass amplitudes are formed once, then spread to the corners.
+// About 40 flops instead of the 64 multiply-adds of the dense 8x8 product.
+template <typename T>
+__device__ __forceinline__ void elem_forces(T s, V2<T> bl, V2<T> br, V2<T> tr, V2<T> tl,
+                                            V2<T> &fbl, V2<T> &fbr, V2<T> &ftr, V2<T> &ftl) {
+  const T a = tr.x - bl.x, b = br.x - tl.x;    // x: diagonal differences
+  const T ay = tr.y - bl.y, by = br.y - tl.y;  // y: diagonal differences
+  const T apb = a + b, ayb = ay - by;
+  const T P = s * fmaT(kst<T>(0), apb, kst<T>(1) * ayb);
+  const T R = s * fmaT(kst<T>(1), apb, kst<T>(0) * ayb);
+  const T Q = s * kst<T>(2) * ((a - b) + (ay + by));
+  const T sh = s * kst<T>(3);
+  const T hx = sh * ((bl.x + tr.x) - (br.x + tl.x));
+  const T hy = sh * ((bl.y + tr.y) - (br.y + tl.y));
+  const T PQ = P + Q, PmQ = P - Q, RQ = R + Q, RmQ = R - Q;
+  fbl = mk2<T>(hx - PQ, hy - RQ);
+  fbr = mk2<T>(PmQ - hx, -(RmQ + hy));
+  ftr = mk2<T>(PQ + hx, RQ + hy);
+  ftl = mk2<T>(-(PmQ + hx), RmQ - hy);
+}
+
 // Point preconditioners computed on the fly from the node's four element
 // scales (same argument order as node_apply).
 //  JACOBI: z = r / diag, diag_i = sum_e s_e Ke_ii, fixed -> 1, floor 1e-20

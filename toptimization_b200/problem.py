@@ -64,7 +64,7 @@ class Problem:
     save_interval: int
     output_format: Literal["png", "vtk"]
     precision: str = "fp64"
-    inner_tol: float = 1e-4
+    inner_tol: float = 1e-3
     max_outer_iter: int = 50
 
     n_nodes: int = field(init=False)
@@ -148,7 +148,7 @@ def problem_from_dict(raw: dict) -> Problem:
         save_interval=int(out.get("save_interval", 10)),
         output_format=output_format,
         precision=precision,
-        inner_tol=float(sol.get("inner_tolerance", 1e-4)),
+        inner_tol=float(sol.get("inner_tolerance", 1e-3)),
         max_outer_iter=int(sol.get("max_outer_iterations", 50)),
     )
 
