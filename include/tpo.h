@@ -68,6 +68,21 @@ enum {
   TPO_PRECISION_MIXED = 1  /* FP32 inner PCG inside FP64 iterative refinement */
 };
 
+/* PCG recurrence. AUTO: one launch per iteration (Chronopoulos-Gear form,
+ * one global reduction) for the plain FP64 solve with a point preconditioner
+ * (none, Jacobi, nodal block); two launches otherwise (element-block
+ * preconditioner, mixed form). STANDARD: the reference's own recurrence
+ * (fem/solver.py:27-159), two launches per iteration. SINGLE: the one-launch
+ * form; TPO_ERR_ARGS for the element-block preconditioner or the mixed form
+ * (its s = K p recurrence is not kept accurately in FP32 storage). Both forms
+ * give the same iterates in exact arithmetic and use the reference's stop,
+ * breakdown and beta rules. */
+enum {
+  TPO_RECURRENCE_AUTO = 0,
+  TPO_RECURRENCE_STANDARD = 1,
+  TPO_RECURRENCE_SINGLE = 2
+};
+
 typedef struct tpo_grid {
   int32_t nelx, nely;
   double e_min;    /* SIMP floor: scale = e_min + rho^penalty (1 - e_min) */
@@ -85,6 +100,7 @@ typedef struct tpo_solve_cfg {
   int32_t max_outer;    /* mixed: refinement steps */
   int32_t poll_every;   /* iterations between host checks of the device status
                            (0 = library default); no effect on results */
+  int32_t recurrence;   /* TPO_RECURRENCE_*: how an iteration is organised */
 } tpo_solve_cfg;
 
 typedef struct tpo_solve_result {
@@ -209,6 +225,9 @@ typedef struct tpo_profile {
   int64_t apply_launches;   /* stiffness kernel of tpo_matvec_* / tpo_apply_stiffness_* */
   double apply_ms;
   int64_t apply_bytes;
+  int64_t step_launches;    /* one-launch PCG iteration kernel (TPO_RECURRENCE_SINGLE) */
+  double step_ms;
+  int64_t step_bytes;
 } tpo_profile;
 int tpo_profile_enable(int on);
 int tpo_profile_reset(void);

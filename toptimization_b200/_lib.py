@@ -36,7 +36,8 @@ class TpoGrid(ctypes.Structure):
 class TpoSolveCfg(ctypes.Structure):
     _fields_ = [("precond", c_int32), ("precision", c_int32), ("max_iter", c_int32),
                 ("warm_start", c_int32), ("tol", c_double), ("f_norm_sq", c_double),
-                ("inner_tol", c_double), ("max_outer", c_int32), ("poll_every", c_int32)]
+                ("inner_tol", c_double), ("max_outer", c_int32), ("poll_every", c_int32),
+                ("recurrence", c_int32)]
 
 
 class TpoSolveResult(ctypes.Structure):
@@ -49,7 +50,9 @@ class TpoProfile(ctypes.Structure):
                 ("update_launches", ctypes.c_int64), ("update_ms", c_double),
                 ("dir_bytes", ctypes.c_int64), ("update_bytes", ctypes.c_int64),
                 ("launches", ctypes.c_int64), ("apply_launches", ctypes.c_int64),
-                ("apply_ms", c_double), ("apply_bytes", ctypes.c_int64)]
+                ("apply_ms", c_double), ("apply_bytes", ctypes.c_int64),
+                ("step_launches", ctypes.c_int64), ("step_ms", c_double),
+                ("step_bytes", ctypes.c_int64)]
 
 
 _PD = POINTER(c_double)

@@ -18,6 +18,7 @@
 #include "common.cuh"
 #include "design.cuh"
 #include "pcg.cuh"
+#include "cgstep.cuh"
 #include "stencil.cuh"
 #include "tpo.h"
 
@@ -84,7 +85,7 @@ int need_stiffness(int *dev) {
 // 64 multiply-adds). The four constants are read off Ke's entries and the
 // decomposition is checked against every entry; a Ke that does not have this
 // structure is rejected. kst = {d11/4, d12/4, d33/4, ch}.
-int stiffness_structure(const double ke[64], double kst[4]) {
+int stiffness_structure(const double ke[64], double kst[6]) {
   const double ch = 0.5 * (ke[0] + ke[4]);
   const double d12 = 2.0 * (ke[1] + ke[3]);
   const double d33 = 2.0 * (ke[1] - ke[3]);
@@ -117,6 +118,8 @@ int stiffness_structure(const double ke[64], double kst[4]) {
   kst[1] = 0.25 * d12;
   kst[2] = 0.25 * d33;
   kst[3] = ch;
+  kst[4] = ke[0];  // every diagonal entry (checked above through the structure)
+  kst[5] = ke[1];  // x-y entry of corner 0; corners 1..3 alternate in sign
   return TPO_OK;
 }
 
@@ -205,6 +208,42 @@ template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
   }
 };
 
+// Launch configuration of the one-launch iteration (k_cgstep): a ring of NG
+// staged columns per CTA (3 x 11 KB in FP64: six CTAs fit an SM), a grid of
+// about one full wave.
+template <typename T, typename C, int PRE> struct CgCfg {
+  static constexpr int NG = 3;
+  static constexpr int SMEM = CgGeom<T>::SLOT * NG;
+  static int resident() {
+    static int occ = -1;
+    if (occ < 0) {
+      auto kern = k_cgstep<T, C, PRE, NG>;
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+      int o = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, ST_THREADS, SMEM) !=
+              cudaSuccess || o < 1)
+        o = 1;
+      occ = o;
+    }
+    return occ;
+  }
+  static void plan(int nx, int ny, dim3 *grid, int *L) {
+    const int rows = (ny + 1 + RPC - 1) / RPC;
+    const int target = sm_count() * resident();
+    int strips = std::max(1, target / rows);
+    int l = std::max(8, (nx + 1 + strips - 1) / strips);
+    strips = (nx + 1 + l - 1) / l;
+    *grid = dim3(rows, strips, 1);
+    *L = l;
+  }
+  static void launch(cudaStream_t st, const CgArgs &a, int nx, int ny) {
+    dim3 grid;
+    int L;
+    plan(nx, ny, &grid, &L);
+    k_cgstep<T, C, PRE, NG><<<grid, ST_THREADS, SMEM, st>>>(a, L);
+  }
+};
+
 struct UpdPlan {
   dim3 grid;
   int L;
@@ -246,10 +285,19 @@ struct PcgWs {
   double *s64, *w64;
   float *s32, *w32;
   double *ra, *rb, *pa, *pb, *ap, *z;          // FP64 solve
-  float *fra, *frb, *fpa, *fpb, *fap, *fz, *fy;  // mixed inner solve
+  float *fra, *frb, *fpa, *fpb, *fap, *fz;       // mixed: FP32 Krylov vectors (u stays FP64)
+  double *wa, *wb, *sa, *sb;                   // one-launch form: w = K M^-1 r, s = K p
+  bool single;                                 // one launch per iteration (k_cgstep)
   int P;
   size_t bytes;
 };
+
+// The one-launch iteration serves the plain FP64 solve with a point
+// preconditioner (its s = K p recurrence is not kept accurately in FP32).
+bool use_single(const tpo_solve_cfg *c) {
+  return c->precond != TPO_PRECOND_BLOCK_JACOBI && c->precision == TPO_PRECISION_FP64 &&
+         c->recurrence != TPO_RECURRENCE_STANDARD;
+}
 
 PcgWs carve_pcg(void *base, const tpo_grid *g, const tpo_solve_cfg *c) {
   const int nx = g->nelx, ny = g->nely, P = pad_pitch(ny);
@@ -261,12 +309,22 @@ PcgWs carve_pcg(void *base, const tpo_grid *g, const tpo_solve_cfg *c) {
   w.P = P;
   w.ctl = cv.take<PcgCtl>(1);
   w.octl = cv.take<OuterCtl>(1);
-  w.part = cv.take<double>(3 * (size_t)max_ctas(g));
+  w.part = cv.take<double>(3 * (size_t)max_ctas(g));  // up to 3 sums per CTA
   w.mask = cv.take<uint8_t>(NN);
   w.u = cv.take<double>(2 * NN);
   w.f = cv.take<double>(2 * NN);
   w.s64 = cv.take<double>(NE);
-  if (mixed) {
+  w.single = use_single(c);
+  if (w.single) {
+    // r, w, s ping-pong; p in place; the solution is u itself
+    w.ra = cv.take<double>(2 * NN);
+    w.rb = cv.take<double>(2 * NN);
+    w.wa = cv.take<double>(2 * NN);
+    w.wb = cv.take<double>(2 * NN);
+    w.sa = cv.take<double>(2 * NN);
+    w.sb = cv.take<double>(2 * NN);
+    w.pa = cv.take<double>(2 * NN);
+  } else if (mixed) {
     w.s32 = cv.take<float>(NE);
     if (block) w.w32 = cv.take<float>(NE);
     w.fra = cv.take<float>(2 * NN);
@@ -275,7 +333,6 @@ PcgWs carve_pcg(void *base, const tpo_grid *g, const tpo_solve_cfg *c) {
     w.fpb = cv.take<float>(2 * NN);
     w.fap = cv.take<float>(2 * NN);
     if (block) w.fz = cv.take<float>(2 * NN);
-    w.fy = cv.take<float>(2 * NN);
   } else {
     if (block) w.w64 = cv.take<double>(NE);
     w.ra = cv.take<double>(2 * NN);
@@ -341,6 +398,7 @@ int prof_events(int slots, cudaEvent_t **out) {
 
 struct LaunchBytes {
   int64_t dir, update;
+  int64_t step = 0;  // nonzero: one launch per iteration, timed by ev[0..1]
 };
 
 // Runs PCG iterations (direction kernel + update kernel) until the device
@@ -388,14 +446,25 @@ int run_iterations(IterFn iter, PcgCtl *dctl, int max_iter, int it0, int chunk, 
   if (prof_slots > 0) {
     // only the launches that did work
     const int real = std::min(final_out->it - it0, std::min(issued, prof_slots));
-    for (int i = 0; i < real; ++i) {
+    if (lb.step > 0) {
+      for (int i = 0; i < real; ++i) {
+        float a = 0.f;
+        TPO_CK(cudaEventElapsedTime(&a, ev[4 * i], ev[4 * i + 1]));
+        g_prof.step_ms += a;
+      }
+      if (real > 0) {
+        g_prof.step_launches += real;
+        g_prof.step_bytes += (int64_t)real * lb.step;
+      }
+    }
+    for (int i = 0; i < real && lb.step == 0; ++i) {
       float a = 0.f, b = 0.f;
       TPO_CK(cudaEventElapsedTime(&a, ev[4 * i], ev[4 * i + 1]));
       TPO_CK(cudaEventElapsedTime(&b, ev[4 * i + 2], ev[4 * i + 3]));
       g_prof.dir_ms += a;
       g_prof.update_ms += b;
     }
-    if (real > 0) {
+    if (real > 0 && lb.step == 0) {
       g_prof.dir_launches += real;
       g_prof.update_launches += real;
       g_prof.dir_bytes += (int64_t)real * lb.dir;
@@ -416,6 +485,15 @@ LaunchBytes launch_bytes(const tpo_grid *g) {
     lb.update = 7 * nd * s + ne * s + nn;  // r, Ap, u, p -> u, r', z; weights
   else
     lb.update = 6 * nd * s + (PRE == TPO_PRECOND_NONE ? 0 : ne * s) + nn;  // u, r, p, Ap -> u, r
+  return lb;
+}
+
+// one-launch iteration: r, w, s, p, x read and written, scales, mask
+template <typename T>
+LaunchBytes step_bytes(const tpo_grid *g) {
+  const int64_t nn = (int64_t)(g->nelx + 1) * (g->nely + 1), nd = 2 * nn;
+  const int64_t ne = (int64_t)g->nelx * g->nely, s = sizeof(T);
+  LaunchBytes lb{0, 0, 10 * nd * s + ne * s + nn};
   return lb;
 }
 
@@ -440,10 +518,10 @@ int pack_inputs(const tpo_grid *g, const PcgWs &w, const double *f, const uint8_
 // Zero every PCG vector once per solve: the kernels write only grid rows, so
 // the pad slots (which the stencils read as zero neighbours) stay zero.
 int zero_vectors(const PcgWs &w, size_t NN, cudaStream_t st) {
-  double *d64[] = {w.ra, w.rb, w.pa, w.pb, w.ap, w.z};
+  double *d64[] = {w.ra, w.rb, w.pa, w.pb, w.ap, w.z, w.wa, w.wb, w.sa, w.sb};
   for (double *p : d64)
     if (p) TPO_CK(cudaMemsetAsync(p, 0, 2 * NN * sizeof(double), st));
-  float *d32[] = {w.fra, w.frb, w.fpa, w.fpb, w.fap, w.fz, w.fy};
+  float *d32[] = {w.fra, w.frb, w.fpa, w.fpb, w.fap, w.fz};
   for (float *p : d32)
     if (p) TPO_CK(cudaMemsetAsync(p, 0, 2 * NN * sizeof(float), st));
   return TPO_OK;
@@ -572,11 +650,12 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
 }
 
 // ----------------------------------------------------------------- mixed PCG
-// One FP32-storage PCG (FP64 arithmetic and dot products) whose recursive
-// residual is replaced by the true FP64 residual f - K u whenever it has
-// dropped by inner_tol since the last replacement ("reliable updates"); the
-// search direction is kept across replacements, so the Krylov space is not
-// discarded. Convergence is decided only on the FP64 residual.
+// One PCG whose Krylov vectors (r, p, Ap, z) are stored in FP32, with FP64
+// arithmetic, dot products and solution u. Its recursive residual is replaced
+// by the true FP64 residual f - K u whenever it has dropped by inner_tol since
+// the last replacement ("reliable updates"); the search direction is kept
+// across replacements, so the Krylov space is not discarded. Convergence is
+// decided only on the FP64 residual.
 template <int PRE>
 int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const double *f,
               const uint8_t *fixed, double *u, const PcgWs &w, tpo_solve_result *out,
@@ -606,7 +685,6 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   rx.a = w.u;
   rx.uw = w.u;
   rx.f = w.f;
-  rx.d = w.fy;
   rx.part = w.part;
   rx.ctl = w.ctl;
   rx.octl = w.octl;
@@ -618,7 +696,7 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   b.P = P;
   b.w = w.w32;
   b.mask = w.mask;
-  b.u = w.fy;
+  b.u = w.u;
   b.ap = w.fap;
   b.pa = w.fpa;
   b.pb = w.fpb;
@@ -647,7 +725,7 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   up.P = P;
   up.s = w.s32;
   up.mask = w.mask;
-  up.u = w.fy;
+  up.u = w.u;
   up.r = w.fra;
   up.ap = w.fap;
   up.pa = w.fpa;
@@ -663,9 +741,10 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
     if (block) {
-      k_blockpre<float, double, false, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
+      k_blockpre<float, double, false, kBlkL, double>
+          <<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     } else {
-      k_update<float, double, PRE><<<upl.grid, UP_THREADS, 0, st>>>(up, upl.L);
+      k_update<float, double, PRE, double><<<upl.grid, UP_THREADS, 0, st>>>(up, upl.L);
     }
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
@@ -675,21 +754,17 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   Poller *pl;
   if ((rc = get_poller(&pl))) return rc;
   const int chunk = c->poll_every > 0 ? c->poll_every : 16;
-  const dim3 fg = flat_grid(2 * NN, 256, sm_count() * 16);
   OuterCtl oh{};
   PcgCtl fin{};
   int status = TPO_SOLVE_MAX_ITER, inner_it = 0;
   for (int k = 0;; ++k) {
-    if (k > 0) {  // fold the FP32 correction into u before the FP64 residual
-      k_accumulate<<<fg, 256, 0, st>>>(2 * NN, w.u, w.fy);
-      TPO_CK_LAUNCH();
-    }
     // block preconditioner: the current residual buffer follows the iteration parity
     rx.out = (block && (inner_it & 1)) ? (void *)w.frb : (void *)w.fra;
     StencilCfg<double, double, M_RESX, PRE>::launch(st, rx, nx, ny);
     TPO_CK_LAUNCH();
     if (block) {
-      k_blockpre<float, double, true, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
+      k_blockpre<float, double, true, kBlkL, double>
+          <<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
       TPO_CK_LAUNCH();
     }
     TPO_CK(cudaMemcpyAsync(&oh, w.octl, sizeof(OuterCtl), cudaMemcpyDeviceToHost, st));
@@ -723,6 +798,87 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   out->updates = inner_it;
   out->outer_iters = oh.it;
   out->rr = oh.rr;
+  return TPO_OK;
+}
+
+// ----------------------------------------------------------------- one-launch PCG
+CgArgs cg_args(const tpo_grid *g, const PcgWs &w) {
+  CgArgs a{};
+  a.nx = g->nelx;
+  a.ny = g->nely;
+  a.P = w.P;
+  a.mask = w.mask;
+  a.s = w.s64;
+  a.ra = w.ra;
+  a.rb = w.rb;
+  a.wa = w.wa;
+  a.wb = w.wb;
+  a.sa = w.sa;
+  a.sb = w.sb;
+  a.p = w.pa;
+  a.x = w.u;
+  a.part = w.part;
+  a.ctl = w.ctl;
+  a.err = &w.ctl->err;
+  return a;
+}
+
+// Plain FP64: r = f - K u, the INIT launch, then one launch per iteration.
+template <int PRE>
+int pcg_single(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const double *f,
+               const uint8_t *fixed, double *u, const PcgWs &w, tpo_solve_result *out,
+               cudaStream_t st, double alpha_reg) {
+  const int nx = g->nelx, ny = g->nely, P = w.P;
+  const double fn = std::sqrt(c->f_norm_sq);
+  const double tol_sq = (c->tol * fn) * (c->tol * fn);
+  int rc = pack_inputs(g, w, f, fixed, u, c->warm_start != 0, st);
+  if (rc) return rc;
+  if ((rc = zero_vectors(w, (size_t)(nx + 1) * P, st))) return rc;
+  k_scales<<<flat_grid((size_t)nx * P, 256, sm_count() * 16), 256, 0, st>>>(
+      nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, nullptr, nullptr, nullptr);
+  TPO_CK_LAUNCH();
+  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, 0.0, c->max_iter, nullptr, 0.0);
+  TPO_CK_LAUNCH();
+
+  TsArgs a{};
+  a.nx = nx;
+  a.ny = ny;
+  a.P = P;
+  a.s = w.s64;
+  a.mask = w.mask;
+  a.a = w.u;
+  a.uw = w.u;
+  a.f = w.f;
+  a.out = w.ra;  // phase 0 reads ra
+  a.part = w.part;
+  a.ctl = w.ctl;
+  a.err = &w.ctl->err;
+  StencilCfg<double, double, M_RES, PRE>::launch(st, a, nx, ny);
+  TPO_CK_LAUNCH();
+
+  const CgArgs ca = cg_args(g, w);
+  CgCfg<double, double, PRE>::launch(st, ca, nx, ny);  // INIT
+  TPO_CK_LAUNCH();
+  auto iter = [&](cudaEvent_t *ev) -> int {
+    if (ev) TPO_CK(cudaEventRecord(ev[0], st));
+    CgCfg<double, double, PRE>::launch(st, ca, nx, ny);
+    TPO_CK_LAUNCH();
+    if (ev) TPO_CK(cudaEventRecord(ev[1], st));
+    return TPO_OK;
+  };
+  PcgCtl fin;
+  const int chunk = c->poll_every > 0 ? c->poll_every : 16;
+  rc = run_iterations(iter, w.ctl, c->max_iter, 0, chunk, st, &fin, step_bytes<double>(g));
+  if (rc) return rc;
+  if ((rc = unpack_solution(g, w, u, st))) return rc;
+  TPO_CK(cudaStreamSynchronize(st));
+  int status = fin.status;
+  if (status == TPO_SOLVE_RUNNING) status = TPO_SOLVE_MAX_ITER;  // max_iter <= 0
+  out->status = status;
+  out->updates = fin.it;
+  out->iters = (status == TPO_SOLVE_CONVERGED) ? fin.it : c->max_iter;
+  out->outer_iters = 1;
+  out->rr = fin.rr;
   return TPO_OK;
 }
 
@@ -809,15 +965,15 @@ int tpo_set_stiffness(const double ke[64], const double ke_inv[64], double alpha
   int dev;
   int rc = current_device(&dev);
   if (rc) return rc;
-  double kst[4];
+  double kst[6];
   rc = stiffness_structure(ke, kst);
   if (rc) return rc;
-  float kf[64], kif[64], kstf[4];
+  float kf[64], kif[64], kstf[6];
   for (int i = 0; i < 64; ++i) {
     kf[i] = (float)ke[i];
     kif[i] = (float)ke_inv[i];
   }
-  for (int i = 0; i < 4; ++i) kstf[i] = (float)kst[i];
+  for (int i = 0; i < 6; ++i) kstf[i] = (float)kst[i];
   TPO_CK(cudaMemcpyToSymbol(c_kst, kst, sizeof(kst)));
   TPO_CK(cudaMemcpyToSymbol(c_kst_f, kstf, sizeof(kstf)));
   TPO_CK(cudaMemcpyToSymbol(c_ke, ke, sizeof(double) * 64));
@@ -908,6 +1064,13 @@ int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_p
     return fail(TPO_ERR_ARGS, "unknown preconditioner %d", c->precond);
   if (c->precision != TPO_PRECISION_FP64 && c->precision != TPO_PRECISION_MIXED)
     return fail(TPO_ERR_ARGS, "unknown precision %d", c->precision);
+  if (c->recurrence < TPO_RECURRENCE_AUTO || c->recurrence > TPO_RECURRENCE_SINGLE)
+    return fail(TPO_ERR_ARGS, "unknown recurrence %d", c->recurrence);
+  if (c->recurrence == TPO_RECURRENCE_SINGLE &&
+      (c->precond == TPO_PRECOND_BLOCK_JACOBI || c->precision != TPO_PRECISION_FP64))
+    return fail(TPO_ERR_ARGS,
+                "the one-launch recurrence serves the FP64 solve with a point preconditioner "
+                "only (not block_jacobi, not the mixed form)");
   if (!(c->tol >= 0.0) || !(c->f_norm_sq >= 0.0))
     return fail(TPO_ERR_ARGS, "tol and f_norm_sq must be >= 0");
   const PcgWs w = carve_pcg(ws, g, c);
@@ -925,6 +1088,16 @@ int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_p
   }
   const double ar = g_alpha_reg[dev];
   const bool mixed = c->precision == TPO_PRECISION_MIXED;
+  if (w.single) {
+    switch (c->precond) {
+      case TPO_PRECOND_NONE:
+        return pcg_single<TPO_PRECOND_NONE>(g, c, rho_phys, f, fixed, u, w, out, st, ar);
+      case TPO_PRECOND_JACOBI:
+        return pcg_single<TPO_PRECOND_JACOBI>(g, c, rho_phys, f, fixed, u, w, out, st, ar);
+      default:
+        return pcg_single<TPO_PRECOND_NODAL_BLOCK>(g, c, rho_phys, f, fixed, u, w, out, st, ar);
+    }
+  }
   switch (c->precond) {
     case TPO_PRECOND_NONE:
       return mixed ? pcg_mixed<TPO_PRECOND_NONE>(g, c, rho_phys, f, fixed, u, w, out, st, ar)

@@ -24,10 +24,12 @@ __constant__ float c_kinv_f[64];
 
 // Square-Q4 structure of Ke: Ke = B0^T D B0 + ch (hx hx^T + hy hy^T), where B0
 // is the strain matrix at the element centre and hx, hy the hourglass modes.
-// {k11, k12, k33, ch} = {D11/4, D12/4, D33/4, ch}, derived from the uploaded Ke
-// and checked against it entry by entry (tpo_set_stiffness).
-__constant__ double c_kst[4];
-__constant__ float c_kst_f[4];
+// {k11, k12, k33, ch, K00, K01} = {D11/4, D12/4, D33/4, ch, Ke[0][0], Ke[0][1]},
+// derived from the uploaded Ke and checked against it entry by entry
+// (tpo_set_stiffness). Every diagonal entry of such a Ke equals K00, and the
+// x-y entry of corner a's 2x2 block is (-1)^a K01.
+__constant__ double c_kst[6];
+__constant__ float c_kst_f[6];
 template <typename T> __device__ __forceinline__ T kst(int i);
 template <> __device__ __forceinline__ double kst<double>(int i) { return c_kst[i]; }
 template <> __device__ __forceinline__ float kst<float>(int i) { return c_kst_f[i]; }
@@ -98,6 +100,7 @@ struct PcgCtl {
   int32_t err;      // nonzero: a bounded wait ran out (TMA pipeline)
   uint32_t counter; // last-CTA ticket
   int32_t since;    // mixed form: iterations since the last residual replacement
+  int32_t phase;    // one-launch iteration: launches done (selects the ping-pong buffers)
 };
 
 // Outer refinement state of the mixed-precision solve.

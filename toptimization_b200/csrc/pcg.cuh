@@ -10,9 +10,13 @@
 // reads the status word first and returns at once when the solve is over, so
 // a host may enqueue more iterations than needed.
 //
-// T is the storage type of the vectors and scales, C the arithmetic type:
-// <double,double> for the plain FP64 solve, <float,double> for the inner
-// solve of the mixed form (FP32 bytes, FP64 arithmetic and dots).
+// T is the storage type of the Krylov vectors (r, p, Ap, z) and scales, C the
+// arithmetic type, X the type of the solution u: <double,double,double> for
+// the plain FP64 solve, <float,double,double> for the mixed form (FP32 bytes
+// for the Krylov vectors, FP64 arithmetic, dot products and solution). u stays
+// FP64 in the mixed form: accumulating it in FP32 between residual
+// replacements injects rounding noise of relative size 2^-24 into every
+// replaced residual, which the iteration then has to remove again.
 //
 // k_tstencil: each CTA owns 120 grid rows (4 warps x 30; a warp's first and
 // last lane are halo rows) and walks a strip of L node columns. Column windows
@@ -56,7 +60,6 @@ struct TsArgs {
   void *out;              // RAW: y; DIR: Ap; RES: r; RESX: inner r (float)
   void *uw;               // RES/RESX: u written back with fixed DOFs zeroed
   const void *f;          // RES/RESX: right-hand side (T)
-  void *d;                // RESX: inner correction, zeroed (float)
   double *part;
   PcgCtl *ctl;
   OuterCtl *octl;
@@ -274,7 +277,6 @@ __global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
         acc[0] += rx * rx + ry * ry;
         const float2 r32 = make_float2((float)rx, (float)ry);
         st2<float>(static_cast<float *>(a.out), node, r32);
-        st2<float>(static_cast<float *>(a.d), node, make_float2(0.f, 0.f));
         if constexpr (PRE != TPO_PRECOND_BLOCK_JACOBI) {
           // the inner kernels see FP32-stored scales: use the same here
           const double2 z = point_precond<double, PRE>(
@@ -393,7 +395,7 @@ __device__ __forceinline__ void finish_update(PcgCtl *ctl, double rz_new, double
   ctl->rz = rz_new;
 }
 
-template <typename T, typename C, int PRE>
+template <typename T, typename C, int PRE, typename X = T>
 __global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
   PcgCtl *ctl = a.ctl;
   if (ctl->status != TPO_SOLVE_RUNNING) return;
@@ -405,7 +407,7 @@ __global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
   const int x0 = blockIdx.y * L;
   const int x1 = min(x0 + L, nx + 1);
   const T *__restrict__ s = static_cast<const T *>(a.s);
-  T *__restrict__ u = static_cast<T *>(a.u);
+  X *__restrict__ u = static_cast<X *>(a.u);
   T *__restrict__ r = static_cast<T *>(a.r);
   const T *__restrict__ ap = static_cast<const T *>(a.ap);
 
@@ -423,7 +425,8 @@ __global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
   ld_s(x0 - 1, ebd, ebu);
   double acc[2] = {0.0, 0.0};
   for (int cb = x0; cb < x1; cb += UB) {
-    V2<T> uv[UB], rv[UB], pv[UB], av[UB];
+    V2<X> uv[UB];
+    V2<T> rv[UB], pv[UB], av[UB];
     C sd[UB], su[UB];
     unsigned m[UB];
 #pragma unroll
@@ -436,7 +439,7 @@ __global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
         if (row_ok) {
           const size_t node = pslot(c, y, P);
           m[k] = a.mask[node];
-          uv[k] = ld2<T>(u, node);
+          uv[k] = ld2<X>(u, node);
           rv[k] = ld2<T>(r, node);
           pv[k] = ld2<T>(p, node);
           av[k] = ld2<T>(ap, node);
@@ -451,11 +454,11 @@ __global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
       ebu = su[k];
       if (c < x1 && row_ok) {
         const size_t node = pslot(c, y, P);
-        const V2<T> un = mk2<T>(T(fmaT(alpha, C(pv[k].x), C(uv[k].x))),
-                                T(fmaT(alpha, C(pv[k].y), C(uv[k].y))));
+        const V2<X> un = mk2<X>(X(fmaT(alpha, C(pv[k].x), C(uv[k].x))),
+                                X(fmaT(alpha, C(pv[k].y), C(uv[k].y))));
         const V2<T> rn = mk2<T>(T(fmaT(-alpha, C(av[k].x), C(rv[k].x))),
                                 T(fmaT(-alpha, C(av[k].y), C(rv[k].y))));
-        st2<T>(u, node, un);
+        st2<X>(u, node, un);
         st2<T>(r, node, rn);
         const V2<C> rc = cvt2<C, T>(rn);
         const V2<C> z = point_precond<C, PRE>(rc, m[k], ead, eau, ebd, ebu);
@@ -491,7 +494,7 @@ struct BlkArgs {
   PcgCtl *ctl;
 };
 
-template <typename T, typename C, bool INIT, int L>
+template <typename T, typename C, bool INIT, int L, typename X = T>
 __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
   PcgCtl *ctl = a.ctl;
   if (ctl->status != TPO_SOLVE_RUNNING) return;
@@ -509,7 +512,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
   const int x0 = blockIdx.y * L;
   const int x1 = min(x0 + L, nx + 1);
   const T *__restrict__ w = static_cast<const T *>(a.w);
-  T *__restrict__ u = static_cast<T *>(a.u);
+  X *__restrict__ u = static_cast<X *>(a.u);
   const T *__restrict__ ap = static_cast<const T *>(a.ap);
   T *__restrict__ z = static_cast<T *>(a.z);
 
@@ -523,7 +526,8 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
 
   struct Raw {
     C wd, wu;
-    V2<T> r, ap, u, p;
+    V2<T> r, ap, p;
+    V2<X> u;
     unsigned m;
   };
   const V2<T> tz = mk2<T>(T(0), T(0));
@@ -536,7 +540,8 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
       R.wu = C(w[e]);
     }
     R.m = 0;
-    R.r = R.ap = R.u = R.p = tz;
+    R.r = R.ap = R.p = tz;
+    R.u = mk2<X>(X(0), X(0));
     if (row_ok && c >= 0 && c <= nx) {
       const size_t node = pslot(c, y, P);
       R.m = a.mask[node];
@@ -544,7 +549,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
       if (!INIT) {
         R.ap = ld2<T>(ap, node);
         if (own_row && c >= x0 && c < x1) {
-          R.u = ld2<T>(u, node);
+          R.u = ld2<X>(u, node);
           R.p = ld2<T>(p, node);
         }
       }
@@ -568,8 +573,8 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
                                 T(fmaT(-alpha, C(cur.ap.y), rn.y)));
         rn = cvt2<C, T>(rs);
         if (own_row && c >= x0 && c < x1) {
-          st2<T>(u, node, mk2<T>(T(fmaT(alpha, C(cur.p.x), C(cur.u.x))),
-                                 T(fmaT(alpha, C(cur.p.y), C(cur.u.y)))));
+          st2<X>(u, node, mk2<X>(X(fmaT(alpha, C(cur.p.x), C(cur.u.x))),
+                                 X(fmaT(alpha, C(cur.p.y), C(cur.u.y)))));
           st2<T>(r_dst, node, rs);
         }
       }
@@ -683,6 +688,7 @@ __global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rupd2, int max_ite
   ctl->first = 1;
   ctl->cont = 0;
   ctl->since = 0;
+  ctl->phase = 0;
   ctl->err = 0;
   ctl->counter = 0u;
   if (octl) {
@@ -694,11 +700,5 @@ __global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rupd2, int max_ite
   }
 }
 
-// mixed form: u += y (FP32 correction accumulated since the last replacement)
-__global__ void k_accumulate(size_t n2, double *__restrict__ u, const float *__restrict__ y) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2;
-       i += (size_t)gridDim.x * blockDim.x)
-    u[i] += (double)y[i];
-}
 
 }  // namespace tpo

@@ -15,9 +15,16 @@ start, breakdown test and returned iteration count are the reference's:
 
 Preconditioners: "jacobi", "block_jacobi" (the reference's element-block
 form), "nodal_block_jacobi" (2x2 nodal blocks, new) and "none".
-Precisions: "fp64" (plain) and "mixed" (FP32 inner PCG to `inner_tol` inside
-FP64 iterative refinement to `tol`; FP64 stays for the outer residual, every
-dot product, alpha/beta).
+Recurrence: "auto" (one kernel launch per iteration, in the Chronopoulos-Gear
+form with a single global reduction, for the plain FP64 solve with a point
+preconditioner; the element-block preconditioner and the mixed form keep two),
+"standard" (the reference's own recurrence, two launches per iteration) or
+"single" (force the one-launch form). The two recurrences produce the same
+iterates in exact arithmetic.
+Precisions: "fp64" (plain) and "mixed" (Krylov vectors r, p, Ap stored in
+FP32, FP64 arithmetic, dot products, alpha/beta and solution u; the recursive
+residual is replaced by the FP64 residual f - K u whenever it has dropped by
+`inner_tol`, and convergence to `tol` is decided on that FP64 residual).
 """
 
 from __future__ import annotations
@@ -27,6 +34,9 @@ from dataclasses import dataclass
 import torch
 
 from .. import _lib
+
+
+RECURRENCE = {"auto": 0, "standard": 1, "single": 2}  # TPO_RECURRENCE_*
 
 
 @dataclass
@@ -49,18 +59,24 @@ class PCGSolver:
                  f_norm_sq: float, *, preconditioner: str = "jacobi",
                  precision: str = "fp64", max_iter: int = 2000, tol: float = 1e-8,
                  inner_tol: float = 1e-4, max_outer: int = 50, poll_every: int = 0,
-                 device=None):
+                 recurrence: str = "auto", device=None):
         if preconditioner not in _lib.PRECOND:
             raise ValueError(f"unknown preconditioner {preconditioner!r}")
         if precision not in _lib.PRECISION:
             raise ValueError(f"unknown precision {precision!r}")
+        if recurrence not in RECURRENCE:
+            raise ValueError(f"unknown recurrence {recurrence!r}")
+        if recurrence == "single" and (preconditioner == "block_jacobi" or precision != "fp64"):
+            raise ValueError("the one-launch recurrence serves the FP64 solve with a point "
+                             "preconditioner only")
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
         self.grid = _lib.grid(nelx, nely, e_min, penalty)
         self.cfg = _lib.TpoSolveCfg(
             precond=_lib.PRECOND[preconditioner], precision=_lib.PRECISION[precision],
             max_iter=int(max_iter), warm_start=1, tol=float(tol), f_norm_sq=float(f_norm_sq),
-            inner_tol=float(inner_tol), max_outer=int(max_outer), poll_every=int(poll_every))
+            inner_tol=float(inner_tol), max_outer=int(max_outer), poll_every=int(poll_every),
+            recurrence=RECURRENCE[recurrence])
         nbytes = _lib.load().tpo_pcg_workspace_bytes(self.grid, self.cfg)
         self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
 

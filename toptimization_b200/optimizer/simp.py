@@ -110,6 +110,7 @@ class SimpDesign:
                                 max_iter=pr.max_cg_iter, tol=pr.cg_tol,
                                 inner_tol=getattr(pr, "inner_tol", 1e-4),
                                 max_outer=getattr(pr, "max_outer_iter", 50),
+                                recurrence=getattr(pr, "recurrence", "auto"),
                                 poll_every=poll_every, device=dev)
         self.sens_ws = K.sensitivity_workspace(self.grid, dev)
         self.oc_ws = oc_mod.oc_workspace(self.grid, dev)

@@ -9,11 +9,13 @@ Numbering conventions (reference `src/toptimization/problem.py:167-173,314-315`)
   3D node (ix, iy, iz)  -> ix*(nely+1)*(nelz+1) + iy*(nelz+1) + iz
   DOF of node n, axis d -> dim*n + d      (d: x=0, y=1, z=2)
 
-Two solver options have no counterpart in the reference and are accepted on
+Three solver options have no counterpart in the reference and are accepted on
 top of its schema: `solver.preconditioner: nodal_block_jacobi` (2x2 nodal
-block-Jacobi) and `solver.precision: fp64|mixed` (plain FP64 PCG, or an FP32
-inner PCG inside FP64 iterative refinement, with `solver.inner_tolerance` and
-`solver.max_outer_iterations`).
+block-Jacobi), `solver.precision: fp64|mixed` (plain FP64 PCG, or a PCG on
+FP32-stored vectors with FP64 residual replacement, with
+`solver.inner_tolerance` and `solver.max_outer_iterations`) and
+`solver.recurrence: auto|standard|single` (one kernel launch per PCG
+iteration, or the reference's own two-step recurrence).
 """
 
 from __future__ import annotations
@@ -27,6 +29,7 @@ import yaml
 
 PRECONDITIONERS = ("jacobi", "block_jacobi", "nodal_block_jacobi", "none")
 PRECISIONS = ("fp64", "mixed")
+RECURRENCES = ("auto", "standard", "single")
 _AXIS = {"x": 0, "y": 1, "z": 2}
 
 
@@ -66,6 +69,7 @@ class Problem:
     precision: str = "fp64"
     inner_tol: float = 1e-3
     max_outer_iter: int = 50
+    recurrence: str = "auto"
 
     n_nodes: int = field(init=False)
     n_dofs: int = field(init=False)
@@ -119,6 +123,13 @@ def problem_from_dict(raw: dict) -> Problem:
     precision = sol.get("precision", "fp64")
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision}")
+    recurrence = sol.get("recurrence", "auto")
+    if recurrence not in RECURRENCES:
+        raise ValueError(
+            f"recurrence must be 'auto', 'standard' or 'single', got {recurrence}")
+    if recurrence == "single" and (preconditioner == "block_jacobi" or precision != "fp64"):
+        raise ValueError("recurrence 'single' needs precision fp64 and a point "
+                         "preconditioner (jacobi, nodal_block_jacobi or none)")
     output_format = out.get("format", "png")
     if output_format not in ("png", "vtk"):
         raise ValueError(f"output format must be 'png' or 'vtk', got {output_format}")
@@ -150,6 +161,7 @@ def problem_from_dict(raw: dict) -> Problem:
         precision=precision,
         inner_tol=float(sol.get("inner_tolerance", 1e-3)),
         max_outer_iter=int(sol.get("max_outer_iterations", 50)),
+        recurrence=recurrence,
     )
 
 
