@@ -233,6 +233,78 @@ int tpo_profile_enable(int on);
 int tpo_profile_reset(void);
 int tpo_profile_read(tpo_profile *out);
 
+/* ---- batched designs -------------------------------------------------------
+ * Many independent designs (uneven sizes) advance together: every kernel step
+ * of an OC iteration (filter, scales, PCG, sensitivity, OC bisection) is ONE
+ * launch over all active designs, each design's CTAs found through a job
+ * table. No reference counterpart: the reference runs one problem per process
+ * (optimizer/simp.py:19-312, module-global Taichi fields in fem/fields.py).
+ * The per-design work is that of one OC iteration of the reference loop with
+ * the mixed-precision PCG and the density filter; a design's launch geometry
+ * depends only on its own size and the batch's strip lengths, so its results
+ * do not depend on which other designs share the batch.
+ * Memory: the library allocates no device memory. The caller gives a batch
+ * workspace (tpo_batch_workspace_bytes) and, per design, a design workspace
+ * (tpo_batch_design_workspace_bytes) that holds that design's resident state
+ * until it is removed. Host bookkeeping lives in the opaque tpo_batch. */
+typedef struct tpo_batch tpo_batch;
+
+typedef struct tpo_batch_cfg {
+  int32_t precond;       /* TPO_PRECOND_NONE / JACOBI / NODAL_BLOCK */
+  int32_t precision;     /* TPO_PRECISION_MIXED */
+  int32_t use_graph;     /* nonzero: each OC iteration is one CUDA graph launch (a while
+                            node runs the PCG loop on the device); 0: host-polled loop */
+  int32_t stencil_cols;  /* columns per CTA of the stencil kernels (0: default 16) */
+  int32_t update_cols;   /* columns per CTA of the update kernel (0: default 8) */
+  int32_t pad;
+} tpo_batch_cfg;
+
+typedef struct tpo_batch_design {
+  int32_t nelx, nely;
+  double e_min, penalty;
+  double volfrac, move;  /* OC (reference optimizer/oc.py:21-93) */
+  double rmin;           /* density filter radius, <= 16 */
+  double tol;            /* stop when it > 5 and change < tol (0: run max_oc_iter) */
+  double cg_tol;         /* FP64 residual stop ||f - K u|| < cg_tol ||f|| */
+  double inner_tol;      /* residual replacement when the FP32 residual drops by this */
+  double f_norm_sq;      /* ||f||^2 */
+  double rho0;           /* initial uniform density */
+  int32_t max_oc_iter;   /* OC iterations to run */
+  int32_t max_cg_iter;   /* PCG iterations per solve */
+  int32_t max_outer;     /* FP64 residual evaluations per solve */
+  int32_t pad;
+} tpo_batch_design;
+
+/* byte offsets, inside a design workspace, of the caller-visible fields:
+ * rho (design density, nelx*nely, element ex*nely+ey), rho_phys (filtered),
+ * u (displacement, 2*(nelx+1)*(nely+1), reference DOF numbering) and hist
+ * (max_oc_iter rows of 6 doubles: compliance, volume, change, PCG iterations,
+ * FP64 residual evaluations, PCG status). All FP64. */
+typedef struct tpo_batch_layout {
+  size_t rho, rho_phys, u, hist;
+} tpo_batch_layout;
+
+size_t tpo_batch_workspace_bytes(int32_t max_designs);
+size_t tpo_batch_design_workspace_bytes(const tpo_batch_design *d, tpo_batch_layout *layout);
+int tpo_batch_create(int32_t max_designs, const tpo_batch_cfg *cfg, void *ws, size_t ws_bytes,
+                     tpo_batch **out);
+int tpo_batch_destroy(tpo_batch *b);
+/* Admits a design (f: its load vector, fixed: its per-node fixed mask, both
+ * device arrays in reference numbering, read during the call only). Blocks
+ * on the stream. */
+int tpo_batch_add(tpo_batch *b, const tpo_batch_design *d, const double *f, const uint8_t *fixed,
+                  void *design_ws, size_t design_ws_bytes, tpo_stream s, int32_t *slot_out);
+/* Releases a slot (its workspace may be reused once this returns). */
+int tpo_batch_remove(tpo_batch *b, int32_t slot);
+int tpo_batch_set_tiles(tpo_batch *b, int32_t stencil_cols, int32_t update_cols);
+/* One OC iteration of every active design; blocks until it is done. */
+int tpo_batch_oc_iteration(tpo_batch *b, tpo_stream s);
+/* Per slot 0..n-1: OC iterations done (-1: empty slot) and whether more remain. */
+int tpo_batch_states(tpo_batch *b, int32_t n, int32_t *it_out, int32_t *active_out);
+/* Device time of `steps` PCG steps with the current tiles (for the autotuner;
+ * advances the designs' PCG state, so use a scratch batch). */
+int tpo_batch_time_steps(tpo_batch *b, int32_t steps, tpo_stream s, float *ms_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,7 +55,26 @@ class TpoProfile(ctypes.Structure):
                 ("step_bytes", ctypes.c_int64)]
 
 
+class TpoBatchCfg(ctypes.Structure):
+    _fields_ = [("precond", c_int32), ("precision", c_int32), ("use_graph", c_int32),
+                ("stencil_cols", c_int32), ("update_cols", c_int32), ("pad", c_int32)]
+
+
+class TpoBatchDesign(ctypes.Structure):
+    _fields_ = [("nelx", c_int32), ("nely", c_int32), ("e_min", c_double),
+                ("penalty", c_double), ("volfrac", c_double), ("move", c_double),
+                ("rmin", c_double), ("tol", c_double), ("cg_tol", c_double),
+                ("inner_tol", c_double), ("f_norm_sq", c_double), ("rho0", c_double),
+                ("max_oc_iter", c_int32), ("max_cg_iter", c_int32), ("max_outer", c_int32),
+                ("pad", c_int32)]
+
+
+class TpoBatchLayout(ctypes.Structure):
+    _fields_ = [("rho", c_size_t), ("rho_phys", c_size_t), ("u", c_size_t), ("hist", c_size_t)]
+
+
 _PD = POINTER(c_double)
+_PI = POINTER(c_int32)
 _SIGS = {
     "tpo_version": (c_int, []),
     "tpo_last_error_string": (ctypes.c_char_p, []),
@@ -88,6 +107,19 @@ _SIGS = {
     "tpo_profile_enable": (c_int, [c_int]),
     "tpo_profile_reset": (c_int, []),
     "tpo_profile_read": (c_int, [POINTER(TpoProfile)]),
+    "tpo_batch_workspace_bytes": (c_size_t, [c_int32]),
+    "tpo_batch_design_workspace_bytes": (c_size_t, [POINTER(TpoBatchDesign),
+                                                    POINTER(TpoBatchLayout)]),
+    "tpo_batch_create": (c_int, [c_int32, POINTER(TpoBatchCfg), c_void_p, c_size_t,
+                                 POINTER(c_void_p)]),
+    "tpo_batch_destroy": (c_int, [c_void_p]),
+    "tpo_batch_add": (c_int, [c_void_p, POINTER(TpoBatchDesign), c_void_p, c_void_p, c_void_p,
+                              c_size_t, c_void_p, _PI]),
+    "tpo_batch_remove": (c_int, [c_void_p, c_int32]),
+    "tpo_batch_set_tiles": (c_int, [c_void_p, c_int32, c_int32]),
+    "tpo_batch_oc_iteration": (c_int, [c_void_p, c_void_p]),
+    "tpo_batch_states": (c_int, [c_void_p, c_int32, _PI, _PI]),
+    "tpo_batch_time_steps": (c_int, [c_void_p, c_int32, c_void_p, POINTER(ctypes.c_float)]),
 }
 
 _lock = threading.Lock()
@@ -163,5 +195,6 @@ def profile_read() -> dict:
 
 
 __all__ = ["load", "check", "grid", "ptr", "stream_handle", "ensure_stiffness", "TpoGrid",
-           "TpoSolveCfg", "TpoSolveResult", "TpoError", "PRECOND", "PRECISION", "SOLVE_STATUS",
+           "TpoSolveCfg", "TpoSolveResult", "TpoBatchCfg", "TpoBatchDesign", "TpoBatchLayout",
+           "TpoError", "PRECOND", "PRECISION", "SOLVE_STATUS",
            "exported_symbols", "c_float", "c_uint8"]

@@ -551,7 +551,7 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
       nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, nullptr, block ? w.w64 : nullptr,
       nullptr);
   TPO_CK_LAUNCH();
-  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, 0.0, c->max_iter, nullptr, 0.0);
+  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, 0.0, c->max_iter, nullptr, 0.0, 0);
   TPO_CK_LAUNCH();
 
   TsArgs a{};
@@ -673,7 +673,8 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
       nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, w.s32, nullptr,
       block ? w.w32 : nullptr);
   TPO_CK_LAUNCH();
-  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, delta * delta, c->max_iter, w.octl, tol_sq);
+  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, delta * delta, c->max_iter, w.octl, tol_sq,
+                              c->max_outer);
   TPO_CK_LAUNCH();
 
   TsArgs rx{};
@@ -837,7 +838,7 @@ int pcg_single(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, con
   k_scales<<<flat_grid((size_t)nx * P, 256, sm_count() * 16), 256, 0, st>>>(
       nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, nullptr, nullptr, nullptr);
   TPO_CK_LAUNCH();
-  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, 0.0, c->max_iter, nullptr, 0.0);
+  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, 0.0, c->max_iter, nullptr, 0.0, 0);
   TPO_CK_LAUNCH();
 
   TsArgs a{};
@@ -1268,3 +1269,6 @@ int tpo_oc_update(const tpo_grid *g, double volfrac, double move, const double *
 }
 
 }  // extern "C"
+
+// batched designs (tpo_batch_*): host side, same translation unit
+#include "batch_host.cuh"

@@ -1,0 +1,267 @@
+// Batched designs: one launch per kernel step covers every design of a batch.
+//
+// Each design occupies a slot with a device record (BDesign) holding its
+// sizes, parameters, its resident state (design and physical density,
+// sensitivities, displacement, the padded PCG vectors of the mixed form, the
+// control blocks of the PCG, the OC bisection and the compliance sum) and its
+// OC-iteration history. A batched kernel is launched with a 1-D grid; every
+// kernel kind has a job table that maps a contiguous range of CTAs to one
+// design and gives that design's local launch geometry (gx x gy CTAs). A CTA
+// finds its job by binary search over the range starts, derives its local
+// block (bx, by) and runs the same device code as the single-design kernel
+// (tstencil_run, update_run, filter_run, ...). Reductions are per design: each
+// design has its own partial-sum buffer and ticket counter, and its last CTA
+// finishes its step.
+//
+// A design's launch geometry depends only on its own size and on the batch's
+// tile parameters, never on the other designs in the batch, so a design's
+// arithmetic (and its reduction order) is the same alone and in any mix.
+//
+// One OC iteration of the batch (reference optimizer/simp.py:141-219, per
+// design): density filter -> SIMP scales -> control init -> PCG (mixed form:
+// FP64 residual replacement, then steps of direction + update) until every
+// design's solve has stopped -> displacement unpack -> sensitivity and
+// compliance -> dc filter -> OC bisection steps -> final OC update ->
+// bookkeeping (history row, iteration count, stop rule).
+#pragma once
+
+#include "common.cuh"
+#include "design.cuh"
+#include "layout.cuh"
+#include "pcg.cuh"
+
+namespace tpo {
+
+// device record of one design slot
+struct BDesign {
+  int nx, ny, P, active;       // active: OC iterations remain
+  int it, max_it, R, max_cg;   // OC iterations done / requested, filter radius, PCG cap
+  int max_outer, ctas_part, pad0, pad1;
+  double e_min, pen, volfrac, move, rmin, tol;  // tol: early stop on change (0: none)
+  double tol_sq, rupd2;        // PCG stop (true residual) and replacement thresholds
+  // compact fields, reference numbering
+  double *rho, *rho_phys, *dc, *dc_filt, *u;
+  double *hist;                // max_it rows of kBatchHist values
+  // padded PCG state of the mixed form
+  uint8_t *mask;
+  double *up, *fp, *s64;
+  float *s32, *fr, *fpa, *fpb, *fap;
+  PcgCtl *ctl;
+  OuterCtl *octl;
+  double *part;
+  // OC bisection and compliance sum
+  OcCtl *oc;
+  double *ocpart;
+  SumCtl *sc;
+  double *spart;
+  double *scal;                // [0] compliance, [1..4] OC result (change, volume, lambda, steps)
+};
+
+// history row per OC iteration: compliance, volume, change, PCG iterations,
+// FP64 residual evaluations, PCG status
+constexpr int kBatchHist = 6;
+
+struct BJob {
+  int cta0;    // first CTA of this design in the launch
+  int gx, gy;  // local grid
+  int slot;
+  int L;       // strip length (stencil / update kinds)
+  int pad;
+};
+
+__device__ __forceinline__ const BJob &find_job(const BJob *__restrict__ jobs, int n) {
+  int lo = 0, hi = n - 1;
+  const int b = (int)blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].cta0 <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return jobs[lo];
+}
+
+// ---------------------------------------------------------------- kernels
+// density filter (which = 0: rho -> rho_phys) or dc filter (which = 1: dc -> dc_filt)
+__global__ void __launch_bounds__(F_THREADS)
+    kb_filter(const BJob *jobs, int nj, const BDesign *ds, int which) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  const int loc = blockIdx.x - J.cta0;
+  const double *x = which ? D.dc : D.rho;
+  double *out = which ? D.dc_filt : D.rho_phys;
+  filter_run<F_DENSITY>(D.nx, D.ny, D.rmin, D.R, x, nullptr, out, nullptr, nullptr, 0.0, 0.0,
+                        loc % J.gx, loc / J.gx);
+}
+
+__global__ void kb_scales(const BJob *jobs, int nj, const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  scales_run(D.nx, D.ny, D.P, D.rho_phys, D.e_min, D.pen, 0.0, D.s64, D.s32, nullptr, nullptr,
+             blockIdx.x - J.cta0, J.gx);
+}
+
+// one thread per slot: PCG and OC control blocks of a new OC iteration
+__global__ void kb_init(BDesign *ds, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const BDesign &D = ds[i];
+  if (!D.active) return;
+  ctl_init_run(D.ctl, D.tol_sq, D.rupd2, D.max_cg, D.octl, D.tol_sq, D.max_outer);
+  oc_init_run(D.oc);
+}
+
+template <int PRE>
+__global__ void __launch_bounds__(ST_THREADS) kb_resx(const BJob *jobs, int nj, const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  TsArgs a{};
+  a.nx = D.nx;
+  a.ny = D.ny;
+  a.P = D.P;
+  a.s = D.s64;
+  a.mask = D.mask;
+  a.a = D.up;
+  a.uw = D.up;
+  a.f = D.fp;
+  a.out = D.fr;
+  a.part = D.part;
+  a.ctl = D.ctl;
+  a.octl = D.octl;
+  a.err = &D.ctl->err;
+  const int loc = blockIdx.x - J.cta0;
+  tstencil_run<double, double, M_RESX, PRE, 2, 4>(a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy,
+                                                  loc);
+}
+
+template <int PRE>
+__global__ void __launch_bounds__(ST_THREADS) kb_dir(const BJob *jobs, int nj, const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  TsArgs a{};
+  a.nx = D.nx;
+  a.ny = D.ny;
+  a.P = D.P;
+  a.s = D.s32;
+  a.mask = D.mask;
+  a.a = D.fr;
+  a.pa = D.fpa;
+  a.pb = D.fpb;
+  a.out = D.fap;
+  a.part = D.part;
+  a.ctl = D.ctl;
+  a.err = &D.ctl->err;
+  const int loc = blockIdx.x - J.cta0;
+  tstencil_run<float, double, M_DIR, PRE, 2, 4>(a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy,
+                                                loc);
+}
+
+template <int PRE>
+__global__ void __launch_bounds__(UP_THREADS) kb_update(const BJob *jobs, int nj,
+                                                        const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  UpdArgs a{};
+  a.nx = D.nx;
+  a.ny = D.ny;
+  a.P = D.P;
+  a.s = D.s32;
+  a.mask = D.mask;
+  a.u = D.up;
+  a.r = D.fr;
+  a.ap = D.fap;
+  a.pa = D.fpa;
+  a.pb = D.fpb;
+  a.part = D.part;
+  a.ctl = D.ctl;
+  const int loc = blockIdx.x - J.cta0;
+  update_run<float, double, PRE, double>(a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy, loc);
+}
+
+// Is any solve of the batch still going? flag[0] = 1 if so; flag[1] = 1 when
+// the body limit stopped a loop that still had work (an error). Inside a CUDA
+// graph it also sets the while-node condition.
+__global__ void kb_cond(const BDesign *ds, int n, int *flag, unsigned *bodies,
+                        unsigned max_bodies, cudaGraphConditionalHandle h, int use_h) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const BDesign &D = ds[i];
+    if (!D.active) continue;
+    const int st = D.ctl->status;
+    if ((st == TPO_SOLVE_RUNNING || st == SOLVE_NEED_UPDATE) && D.ctl->err == 0) any = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned b = *bodies + 1u;
+    *bodies = b;
+    const int go = any && b < max_bodies;
+    if (any && !go) flag[1] = 1;
+    flag[0] = go;
+    if (use_h) cudaGraphSetConditional(h, go ? 1u : 0u);
+  }
+}
+
+__global__ void kb_unpack(const BJob *jobs, int nj, const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  unpack_nodes_run(D.nx, D.ny, D.P, D.up, D.u, blockIdx.x - J.cta0, J.gx);
+}
+
+__global__ void __launch_bounds__(S_THREADS) kb_sens(const BJob *jobs, int nj, const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  const int loc = blockIdx.x - J.cta0;
+  sensitivity_run(D.nx, D.ny, D.e_min, D.pen, D.rho_phys, D.u, D.dc, D.spart, D.sc, D.scal,
+                  loc % J.gx, loc / J.gx, J.gx * J.gy, loc);
+}
+
+__global__ void __launch_bounds__(OC_THREADS) kb_ocstep(const BJob *jobs, int nj,
+                                                         const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  oc_step_run(D.nx * D.ny, D.volfrac, D.move, D.rho, D.dc_filt, nullptr, D.ocpart, D.oc,
+              blockIdx.x - J.cta0, J.gx);
+}
+
+// the design density is updated in place (each element by the thread that reads it)
+__global__ void __launch_bounds__(OC_THREADS) kb_ocfinal(const BJob *jobs, int nj,
+                                                          const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active) return;
+  oc_final_run(D.nx * D.ny, D.move, D.rho, D.dc_filt, nullptr, D.rho, D.oc, D.scal + 1,
+               blockIdx.x - J.cta0, J.gx);
+}
+
+// one thread per slot: history row, iteration count, stop rule
+// (reference optimizer/simp.py:216-219: stop when it > 5 and change < tol);
+// status[2i..2i+1] = (it, active) for the host, *err |= 1 on a pipeline timeout
+__global__ void kb_finish(BDesign *ds, int n, int *status, int *err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BDesign &D = ds[i];
+  if (!D.active) return;
+  if (D.ctl->err) atomicOr(err, 1);
+  double *h = D.hist + (size_t)D.it * kBatchHist;
+  h[0] = D.scal[0];
+  h[1] = D.scal[2];
+  h[2] = D.scal[1];
+  h[3] = (double)D.ctl->it;
+  h[4] = (double)D.octl->it;
+  h[5] = (double)D.ctl->status;
+  D.it += 1;
+  if (D.it >= D.max_it || (D.tol > 0.0 && D.it > 5 && D.scal[1] < D.tol)) D.active = 0;
+  status[2 * i] = D.it;
+  status[2 * i + 1] = D.active;
+}
+
+}  // namespace tpo

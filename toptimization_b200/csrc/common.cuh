@@ -110,7 +110,7 @@ struct OuterCtl {
   int32_t it;       // residual evaluations so far
   int32_t status;   // TPO_SOLVE_*
   uint32_t counter;
-  int32_t pad;
+  int32_t max_outer;  // residual evaluations allowed (then TPO_SOLVE_MAX_ITER)
 };
 
 struct OcCtl {
@@ -133,11 +133,10 @@ struct SumCtl {
 // when bit k of MAXMASK is set. `part` holds NV*nblocks doubles. All threads
 // of every CTA must call this (no early returns before it).
 template <int NV, unsigned MAXMASK = 0u>
-__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *part, uint32_t *counter) {
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *part, uint32_t *counter,
+                                            int nb, int bid) {
   __shared__ double sm[NV * 32];
   __shared__ int s_last;
-  const int nb = gridDim.x * gridDim.y;
-  const int bid = blockIdx.y * gridDim.x + blockIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #define TPO_RED(k, a, b) (((MAXMASK >> (k)) & 1u) ? fmax((a), (b)) : (a) + (b))
 #pragma unroll
@@ -182,6 +181,12 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *part, uint3
 #undef TPO_RED
   if (threadIdx.x == 0) *counter = 0u;
   return true;
+}
+// over the whole launch grid
+template <int NV, unsigned MAXMASK = 0u>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *part, uint32_t *counter) {
+  return grid_reduce<NV, MAXMASK>(v, part, counter, (int)(gridDim.x * gridDim.y),
+                                  (int)(blockIdx.y * gridDim.x + blockIdx.x));
 }
 
 __device__ __forceinline__ bool finite(double x) { return isfinite(x); }

@@ -20,18 +20,20 @@ constexpr int F_MAXR = 16;
 
 enum FilterMode { F_DENSITY = 0, F_SENS = 1 };
 
+// (bx, by) = (tile row, tile column) of this CTA
 template <int MODE>
-__global__ void __launch_bounds__(F_THREADS)
-    k_filter(int nx, int ny, double rmin, int R, const double *__restrict__ x,
-             const double *__restrict__ rho, double *__restrict__ out,
-             double *__restrict__ s_out, float *__restrict__ s32_out, double e_min,
-             double pen) {
+__device__ __forceinline__ void filter_run(int nx, int ny, double rmin, int R,
+                                           const double *__restrict__ x,
+                                           const double *__restrict__ rho,
+                                           double *__restrict__ out, double *__restrict__ s_out,
+                                           float *__restrict__ s32_out, double e_min, double pen,
+                                           int bx, int by) {
   extern __shared__ double fsm[];
   const int W = 2 * R + 1;
   const int TW = FT + 2 * R;  // staged tile edge
   double *wt = fsm;           // W*W weights
   double *tile = fsm + W * W; // TW*TW values, index tx*TW + ty
-  const int ex0 = blockIdx.y * FT, ey0 = blockIdx.x * FT;
+  const int ex0 = by * FT, ey0 = bx * FT;
 
   for (int k = threadIdx.x; k < W * W; k += blockDim.x) {
     const int dx = k / W - R, dy = k % W - R;
@@ -84,6 +86,15 @@ __global__ void __launch_bounds__(F_THREADS)
     out[e] = o;
   }
 }
+template <int MODE>
+__global__ void __launch_bounds__(F_THREADS)
+    k_filter(int nx, int ny, double rmin, int R, const double *__restrict__ x,
+             const double *__restrict__ rho, double *__restrict__ out,
+             double *__restrict__ s_out, float *__restrict__ s32_out, double e_min,
+             double pen) {
+  filter_run<MODE>(nx, ny, rmin, R, x, rho, out, s_out, s32_out, e_min, pen, blockIdx.x,
+                   blockIdx.y);
+}
 
 // ---------------------------------------------------------------------------
 // Compliance and sensitivity (reference fem/kernels.py:234-272):
@@ -94,12 +105,13 @@ __global__ void __launch_bounds__(F_THREADS)
 constexpr int S_THREADS = 128;
 constexpr int SL = 16;
 
-__global__ void __launch_bounds__(S_THREADS)
-    k_sensitivity(int nx, int ny, double e_min, double pen, const double *__restrict__ rho,
-                  const double *__restrict__ u, double *__restrict__ dc, double *part,
-                  SumCtl *ctl, double *c_out) {
-  const int ey = blockIdx.x * blockDim.x + threadIdx.x;
-  const int x0 = blockIdx.y * SL;
+__device__ __forceinline__ void sensitivity_run(int nx, int ny, double e_min, double pen,
+                                                const double *__restrict__ rho,
+                                                const double *__restrict__ u,
+                                                double *__restrict__ dc, double *part, SumCtl *ctl,
+                                                double *c_out, int bx, int by, int nb, int bid) {
+  const int ey = bx * blockDim.x + threadIdx.x;
+  const int x0 = by * SL;
   const int x1 = min(x0 + SL, nx);
   const size_t ny1 = (size_t)ny + 1;
   double acc[1] = {0.0};
@@ -126,8 +138,15 @@ __global__ void __launch_bounds__(S_THREADS)
       hi = rhi;
     }
   }
-  if (!grid_reduce<1>(acc, part, &ctl->counter)) return;
+  if (!grid_reduce<1>(acc, part, &ctl->counter, nb, bid)) return;
   if (threadIdx.x == 0) *c_out = acc[0];
+}
+__global__ void __launch_bounds__(S_THREADS)
+    k_sensitivity(int nx, int ny, double e_min, double pen, const double *__restrict__ rho,
+                  const double *__restrict__ u, double *__restrict__ dc, double *part,
+                  SumCtl *ctl, double *c_out) {
+  sensitivity_run(nx, ny, e_min, pen, rho, u, dc, part, ctl, c_out, blockIdx.x, blockIdx.y,
+                  gridDim.x * gridDim.y, blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -148,7 +167,7 @@ __device__ __forceinline__ double oc_candidate(double r, double d, double dvv, d
   return fmax(lo, fmin(hi, cand));
 }
 
-__global__ void k_oc_init(OcCtl *ctl) {
+__device__ __forceinline__ void oc_init_run(OcCtl *ctl) {
   ctl->lo = 0.0;
   ctl->hi = 1e9;
   ctl->mid = 0.5 * (0.0 + 1e9);
@@ -159,21 +178,23 @@ __global__ void k_oc_init(OcCtl *ctl) {
   ctl->done = 0;
   ctl->counter = 0u;
 }
+__global__ void k_oc_init(OcCtl *ctl) { oc_init_run(ctl); }
 
-__global__ void __launch_bounds__(OC_THREADS)
-    k_oc_step(int n, double volfrac, double move, const double *__restrict__ rho,
-              const double *__restrict__ dc, const double *__restrict__ dv, double *part,
-              OcCtl *ctl) {
+__device__ __forceinline__ void oc_step_run(int n, double volfrac, double move,
+                                            const double *__restrict__ rho,
+                                            const double *__restrict__ dc,
+                                            const double *__restrict__ dv, double *part,
+                                            OcCtl *ctl, int bx, int gx) {
   if (ctl->done) return;
   const double lam = ctl->mid;
   double acc[2] = {0.0, 0.0};  // sum of new densities, max |change|
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+  for (int e = bx * blockDim.x + threadIdx.x; e < n; e += gx * blockDim.x) {
     const double r = rho[e];
     const double nw = oc_candidate(r, dc[e], dv ? dv[e] : 1.0, lam, move);
     acc[0] += nw;
     acc[1] = fmax(acc[1], fabs(nw - r));
   }
-  if (!grid_reduce<2, 2u>(acc, part, &ctl->counter)) return;
+  if (!grid_reduce<2, 2u>(acc, part, &ctl->counter, gx, bx)) return;
   if (threadIdx.x != 0) return;
   const double chg = acc[1];
   const double vol = acc[0] / n;
@@ -189,20 +210,33 @@ __global__ void __launch_bounds__(OC_THREADS)
   }
 }
 
-__global__ void k_oc_final(int n, double move, const double *rho_in, const double *__restrict__ dc,
-                           const double *__restrict__ dv, double *rho_out, const OcCtl *ctl,
-                           double *result) {
+__global__ void __launch_bounds__(OC_THREADS)
+    k_oc_step(int n, double volfrac, double move, const double *__restrict__ rho,
+              const double *__restrict__ dc, const double *__restrict__ dv, double *part,
+              OcCtl *ctl) {
+  oc_step_run(n, volfrac, move, rho, dc, dv, part, ctl, blockIdx.x, gridDim.x);
+}
+
+__device__ __forceinline__ void oc_final_run(int n, double move, const double *rho_in,
+                                             const double *__restrict__ dc,
+                                             const double *__restrict__ dv, double *rho_out,
+                                             const OcCtl *ctl, double *result, int bx, int gx) {
   const double lam = ctl->last_mid;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+  for (int e = bx * blockDim.x + threadIdx.x; e < n; e += gx * blockDim.x) {
     const double r = rho_in[e];
     rho_out[e] = oc_candidate(r, dc[e], dv ? dv[e] : 1.0, lam, move);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0 && result) {
+  if (bx == 0 && threadIdx.x == 0 && result) {
     result[0] = ctl->change;
     result[1] = ctl->vol;
     result[2] = ctl->last_mid;
     result[3] = (double)ctl->steps;
   }
+}
+__global__ void k_oc_final(int n, double move, const double *rho_in, const double *__restrict__ dc,
+                           const double *__restrict__ dv, double *rho_out, const OcCtl *ctl,
+                           double *result) {
+  oc_final_run(n, move, rho_in, dc, dv, rho_out, ctl, result, blockIdx.x, gridDim.x);
 }
 
 }  // namespace tpo

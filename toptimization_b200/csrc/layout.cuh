@@ -55,16 +55,21 @@ __global__ void k_pack_nodes(int nx, int ny, int P, const double *__restrict__ s
   }
 }
 
-__global__ void k_unpack_nodes(int nx, int ny, int P, const double *__restrict__ src,
-                               double *__restrict__ dst) {
+__device__ __forceinline__ void unpack_nodes_run(int nx, int ny, int P,
+                                                 const double *__restrict__ src,
+                                                 double *__restrict__ dst, int bx, int gx) {
   const size_t total = (size_t)(nx + 1) * (ny + 1);
-  for (size_t n = blockIdx.x * (size_t)blockDim.x + threadIdx.x; n < total;
-       n += (size_t)gridDim.x * blockDim.x) {
+  for (size_t n = bx * (size_t)blockDim.x + threadIdx.x; n < total;
+       n += (size_t)gx * blockDim.x) {
     const int c = (int)(n / (ny + 1)), y = (int)(n % (ny + 1));
     const size_t i = (size_t)c * P + y + LEAD;
     dst[2 * n] = src[2 * i];
     dst[2 * n + 1] = src[2 * i + 1];
   }
+}
+__global__ void k_unpack_nodes(int nx, int ny, int P, const double *__restrict__ src,
+                               double *__restrict__ dst) {
+  unpack_nodes_run(nx, ny, P, src, dst, blockIdx.x, gridDim.x);
 }
 
 template <typename T>

@@ -77,8 +77,11 @@ template <typename T, int MODE> struct TsGeom {
   }
 };
 
+// (bx, by) = (row block, strip) of this CTA, nb / bid = CTAs of the solve and
+// this CTA's index among them (a batched launch runs many solves at once)
 template <typename T, typename C, int MODE, int PRE, int G, int NG>
-__global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
+__device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int by, int nb,
+                                             int bid) {
   using Geo = TsGeom<T, MODE>;
   constexpr int NV = (MODE == M_RAW || MODE == M_DIR) ? 1 : (MODE == M_RES ? 2 : 3);
   constexpr int SLOT = Geo::template slot_bytes<G>();
@@ -97,14 +100,16 @@ __global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
     parity = ctl->it & 1;
   }
   if constexpr (MODE == M_RESX) {
-    if (a.octl->status != TPO_SOLVE_RUNNING) return;
+    // runs only when the inner iteration asked for a residual replacement
+    // (or before the first iteration): a batched launch reaches every solve
+    if (ctl->status != SOLVE_NEED_UPDATE || a.octl->status != TPO_SOLVE_RUNNING) return;
   }
   const int nx = a.nx, ny = a.ny, P = a.P;
-  const int Y0 = blockIdx.x * RPC;
+  const int Y0 = bx * RPC;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int y = Y0 + wid * RPW - 1 + lane;
   const bool own_row = lane >= 1 && lane <= RPW && y <= ny;
-  const int x0 = blockIdx.y * L;
+  const int x0 = by * L;
   const int x1 = min(x0 + L, nx + 1);
   const int cA = x0 - 2;               // first staged column
   const int NC = x1 - cA + 1;          // staged columns cA..x1
@@ -305,7 +310,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
   }
   __syncthreads();  // no warp leaves while thread 0 may still be staging
   uint32_t *counter = (MODE == M_RESX) ? &a.octl->counter : &ctl->counter;
-  if (!grid_reduce<NV>(acc, a.part, counter)) return;
+  if (!grid_reduce<NV>(acc, a.part, counter, nb, bid)) return;
   if (threadIdx.x != 0) return;
   if constexpr (MODE == M_RAW) {
     if (a.result) *a.result = acc[0];
@@ -331,6 +336,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
     const bool cont = o->it > 1;
     if (!finite(acc[0]) || !finite(acc[1]) || !finite(acc[2])) o->status = TPO_SOLVE_NONFINITE;
     else if (acc[0] < o->tol_sq) o->status = TPO_SOLVE_CONVERGED;
+    else if (o->it > o->max_outer) o->status = TPO_SOLVE_MAX_ITER;
     ctl->rmax2 = acc[0];
     ctl->since = 0;
     ctl->rr = acc[2];
@@ -344,8 +350,14 @@ __global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
       }
       ctl->rz = acc[1];
     }
-    ctl->status = (o->status == TPO_SOLVE_RUNNING) ? TPO_SOLVE_RUNNING : TPO_SOLVE_CONVERGED;
+    ctl->status = o->status;  // RUNNING, or the outer solve's end state
   }
+}
+
+template <typename T, typename C, int MODE, int PRE, int G, int NG>
+__global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
+  tstencil_run<T, C, MODE, PRE, G, NG>(a, L, blockIdx.x, blockIdx.y, gridDim.x * gridDim.y,
+                                       blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -396,15 +408,16 @@ __device__ __forceinline__ void finish_update(PcgCtl *ctl, double rz_new, double
 }
 
 template <typename T, typename C, int PRE, typename X = T>
-__global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
+__device__ __forceinline__ void update_run(const UpdArgs &a, int L, int bx, int by, int nb,
+                                           int bid) {
   PcgCtl *ctl = a.ctl;
   if (ctl->status != TPO_SOLVE_RUNNING) return;
   const C alpha = C(ctl->alpha);
   const T *__restrict__ p = static_cast<const T *>((ctl->it & 1) ? a.pa : a.pb);
   const int nx = a.nx, ny = a.ny, P = a.P;
-  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = bx * blockDim.x + threadIdx.x;
   const bool row_ok = y <= ny;
-  const int x0 = blockIdx.y * L;
+  const int x0 = by * L;
   const int x1 = min(x0 + L, nx + 1);
   const T *__restrict__ s = static_cast<const T *>(a.s);
   X *__restrict__ u = static_cast<X *>(a.u);
@@ -467,8 +480,14 @@ __global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
       }
     }
   }
-  if (!grid_reduce<2>(acc, a.part, &ctl->counter)) return;
+  if (!grid_reduce<2>(acc, a.part, &ctl->counter, nb, bid)) return;
   if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
+}
+
+template <typename T, typename C, int PRE, typename X = T>
+__global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
+  update_run<T, C, PRE, X>(a, L, blockIdx.x, blockIdx.y, gridDim.x * gridDim.y,
+                           blockIdx.y * gridDim.x + blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -626,13 +645,14 @@ __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
 // s = e_min + rho^p (1 - e_min) (reference fem/kernels.py:92), its FP32 copy,
 // and the element-block weights w = s / max(s, alpha)^2 (preconditioner.py:55-57).
 // Writes every slot of the padded arrays (pads = 0).
-__global__ void k_scales(int nx, int ny, int P, const double *__restrict__ rho, double e_min,
-                         double pen, double alpha_reg, double *__restrict__ s64,
-                         float *__restrict__ s32, double *__restrict__ w64,
-                         float *__restrict__ w32) {
+__device__ __forceinline__ void scales_run(int nx, int ny, int P, const double *__restrict__ rho,
+                                           double e_min, double pen, double alpha_reg,
+                                           double *__restrict__ s64, float *__restrict__ s32,
+                                           double *__restrict__ w64, float *__restrict__ w32,
+                                           int bx, int gx) {
   const size_t total = (size_t)nx * P;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
-       i += (size_t)gridDim.x * blockDim.x) {
+  for (size_t i = bx * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gx * blockDim.x) {
     const int ex = (int)(i / P), ey = (int)(i % P) - LEAD;
     double s = 0.0, w = 0.0;
     if (ey >= 0 && ey < ny) {
@@ -645,6 +665,12 @@ __global__ void k_scales(int nx, int ny, int P, const double *__restrict__ rho, 
     if (w64) w64[i] = w;
     if (w32) w32[i] = (float)w;
   }
+}
+__global__ void k_scales(int nx, int ny, int P, const double *__restrict__ rho, double e_min,
+                         double pen, double alpha_reg, double *__restrict__ s64,
+                         float *__restrict__ s32, double *__restrict__ w64,
+                         float *__restrict__ w32) {
+  scales_run(nx, ny, P, rho, e_min, pen, alpha_reg, s64, s32, w64, w32, blockIdx.x, gridDim.x);
 }
 
 // element values (compact, T) -> SIMP scales, padded T
@@ -672,8 +698,11 @@ __global__ void k_pad_elems(int nx, int ny, int P, const T *__restrict__ src, T 
   }
 }
 
-__global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rupd2, int max_iter,
-                           OuterCtl *octl, double outer_tol_sq) {
+// Per-solve control state. The mixed form (octl non-null) starts in
+// SOLVE_NEED_UPDATE: its first step is the FP64 residual.
+__device__ __forceinline__ void ctl_init_run(PcgCtl *ctl, double tol_sq, double rupd2,
+                                             int max_iter, OuterCtl *octl, double outer_tol_sq,
+                                             int max_outer) {
   ctl->rz = 0.0;
   ctl->alpha = 0.0;
   ctl->beta = 0.0;
@@ -683,7 +712,7 @@ __global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rupd2, int max_ite
   ctl->rupd2 = rupd2;
   ctl->rmax2 = 0.0;
   ctl->it = 0;
-  ctl->status = TPO_SOLVE_RUNNING;
+  ctl->status = octl ? SOLVE_NEED_UPDATE : TPO_SOLVE_RUNNING;
   ctl->max_iter = max_iter;
   ctl->first = 1;
   ctl->cont = 0;
@@ -697,7 +726,12 @@ __global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rupd2, int max_ite
     octl->it = 0;
     octl->status = TPO_SOLVE_RUNNING;
     octl->counter = 0u;
+    octl->max_outer = max_outer;
   }
+}
+__global__ void k_ctl_init(PcgCtl *ctl, double tol_sq, double rupd2, int max_iter,
+                           OuterCtl *octl, double outer_tol_sq, int max_outer) {
+  ctl_init_run(ctl, tol_sq, rupd2, max_iter, octl, outer_tol_sq, max_outer);
 }
 
 
