@@ -297,8 +297,15 @@ int tpo_batch_add(tpo_batch *b, const tpo_batch_design *d, const double *f, cons
 /* Releases a slot (its workspace may be reused once this returns). */
 int tpo_batch_remove(tpo_batch *b, int32_t slot);
 int tpo_batch_set_tiles(tpo_batch *b, int32_t stencil_cols, int32_t update_cols);
-/* One OC iteration of every active design; blocks until it is done. */
+/* One OC iteration of every active design; blocks until it is done. With
+ * use_graph the iteration is one CUDA graph launch. */
 int tpo_batch_oc_iteration(tpo_batch *b, tpo_stream s);
+/* One round of continuous batching: designs about to start an OC iteration
+ * start it, every design inside its PCG solve advances by one loop body
+ * (one FP64 residual check and 8 PCG steps), and designs whose solve stopped
+ * finish their OC iteration. Designs at different OC iterations share every
+ * launch; none waits for another's solve. Blocks until done. */
+int tpo_batch_round(tpo_batch *b, tpo_stream s);
 /* Per slot 0..n-1: OC iterations done (-1: empty slot) and whether more remain. */
 int tpo_batch_states(tpo_batch *b, int32_t n, int32_t *it_out, int32_t *active_out);
 /* Device time of `steps` PCG steps with the current tiles (for the autotuner;

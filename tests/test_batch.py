@@ -71,3 +71,15 @@ def test_workspace_queries(lib):
     bad = design_struct(p)
     bad.rmin = 17.0
     assert lib.tpo_batch_design_workspace_bytes(bad, None) == 0
+
+
+def test_poisson_stream_is_seeded():
+    from toptimization_b200.serve import poisson_stream
+    a = poisson_stream(400, rate=50.0, seed=5)
+    b = poisson_stream(400, rate=50.0, seed=5)
+    assert [r.arrival for r in a] == [r.arrival for r in b]
+    t = np.array([r.arrival for r in a])
+    assert np.all(np.diff(t) > 0)
+    gaps = np.diff(np.concatenate([[0.0], t]))
+    assert abs(gaps.mean() - 1 / 50.0) < 0.2 / 50.0
+    assert all(64 <= r.problem.nelx <= 1024 for r in a)

@@ -100,3 +100,53 @@ def test_autotune_reports_every_candidate(tpo_built):
     for i in range(2):
         ca, cc = a[i][1]["compliance"], c[i][1]["compliance"]
         assert abs(ca[0] - cc[0]) / ca[0] < 1e-7
+
+
+def test_rounds_and_oc_iterations_agree(tpo_built):
+    """Continuous-batching rounds (each design at its own pace) give the same
+    bits as OC iterations in lock step."""
+    ps = _designs(4, seed=31)
+    a = Batch(4)
+    sa = [a.add(p) for p in ps]
+    a.run(rounds=False)
+    b = Batch(4)
+    sb = [b.add(p) for p in ps]
+    b.run(rounds=True)
+    for i in range(4):
+        assert np.array_equal(a.density(sa[i]), b.density(sb[i]))
+        assert np.array_equal(a.history(sa[i])["compliance"], b.history(sb[i])["compliance"])
+    a.close()
+    b.close()
+
+
+def test_served_results_equal_alone(tpo_built):
+    """Each request's result in the served stream (others arriving and
+    leaving around it) is bit-identical to the same request run alone."""
+    from toptimization_b200.serve import Server, poisson_stream
+    reqs = poisson_stream(6, rate=200.0, seed=3, nelx_range=(64, 160), max_iter=4)
+    srv = Server(max_slots=8, keep_density=True)
+    rep = srv.serve(reqs)
+    srv.close()
+    assert len(rep.completions) == 6 and rep.peak_resident >= 2
+    for c in rep.completions:
+        alone = Batch(1)
+        s = alone.add(reqs[c.rid].problem)
+        alone.run(rounds=True)
+        assert np.array_equal(alone.density(s), c.density)
+        assert alone.history(s)["compliance"][-1] == c.compliance
+        alone.close()
+    summ = rep.summary()
+    assert summ["p50_s"] <= summ["p95_s"] <= summ["p99_s"]
+
+
+def test_admission_respects_the_memory_budget(tpo_built):
+    from toptimization_b200.batch import footprint_bytes
+    from toptimization_b200.serve import Server, poisson_stream
+    reqs = poisson_stream(5, rate=1000.0, seed=4, nelx_range=(64, 96), max_iter=2)
+    fps = sorted(footprint_bytes(r.problem) for r in reqs)
+    budget = fps[-1] + fps[-2]  # any two fit, never three
+    srv = Server(hbm_budget=budget, max_slots=8)
+    rep = srv.serve(reqs)
+    srv.close()
+    assert len(rep.completions) == 5
+    assert rep.peak_resident <= 2 and rep.peak_bytes <= budget

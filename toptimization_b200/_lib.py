@@ -118,6 +118,7 @@ _SIGS = {
     "tpo_batch_remove": (c_int, [c_void_p, c_int32]),
     "tpo_batch_set_tiles": (c_int, [c_void_p, c_int32, c_int32]),
     "tpo_batch_oc_iteration": (c_int, [c_void_p, c_void_p]),
+    "tpo_batch_round": (c_int, [c_void_p, c_void_p]),
     "tpo_batch_states": (c_int, [c_void_p, c_int32, _PI, _PI]),
     "tpo_batch_time_steps": (c_int, [c_void_p, c_int32, c_void_p, POINTER(ctypes.c_float)]),
 }

@@ -134,6 +134,13 @@ class Batch:
         it, active = self.states()
         return bool(active.any())
 
+    def round(self) -> None:
+        """One round of continuous batching (`tpo_batch_round`): every design
+        advances by one PCG loop body or one OC-iteration stage, whatever the
+        OC iteration it is at."""
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.tpo_batch_round(self.handle, _lib.stream_handle()))
+
     def states(self) -> tuple[np.ndarray, np.ndarray]:
         n = self.max_designs
         it = (ctypes.c_int32 * n)()
@@ -141,9 +148,17 @@ class Batch:
         _lib.check(self.lib.tpo_batch_states(self.handle, n, it, act))
         return np.frombuffer(it, dtype=np.int32).copy(), np.frombuffer(act, dtype=np.int32).copy()
 
-    def run(self) -> None:
-        while self.step():
-            pass
+    def run(self, rounds: bool = False) -> None:
+        """Run every design to its end, by OC iterations (all designs step
+        together) or by rounds (each design at its own pace)."""
+        if not rounds:
+            while self.step():
+                pass
+            return
+        while True:
+            self.round()
+            if not self.states()[1].any():
+                return
 
     # -- results
     def _view(self, slot: int, off: int, count: int) -> torch.Tensor:

@@ -17,12 +17,15 @@
 // tile parameters, never on the other designs in the batch, so a design's
 // arithmetic (and its reduction order) is the same alone and in any mix.
 //
-// One OC iteration of the batch (reference optimizer/simp.py:141-219, per
-// design): density filter -> SIMP scales -> control init -> PCG (mixed form:
-// FP64 residual replacement, then steps of direction + update) until every
-// design's solve has stopped -> displacement unpack -> sensitivity and
-// compliance -> dc filter -> OC bisection steps -> final OC update ->
-// bookkeeping (history row, iteration count, stop rule).
+// One OC iteration of a design (reference optimizer/simp.py:141-219) runs in
+// three phases. PRE: density filter -> SIMP scales -> control init. SOLVE:
+// PCG of the mixed form (FP64 residual replacement, then steps of direction
+// + update) until its solve stops. POST: displacement unpack -> sensitivity
+// and compliance -> dc filter -> OC bisection and update -> bookkeeping
+// (history row, iteration count, stop rule), back to PRE. Every batched
+// kernel acts only on the designs in its phase, so designs at different
+// stages share the same launches (continuous batching), and a design's own
+// sequence of operations is the same whatever the others are doing.
 #pragma once
 
 #include "common.cuh"
@@ -33,10 +36,13 @@
 namespace tpo {
 
 // device record of one design slot
+// phases of a design within its current OC iteration
+enum BPhase { PH_PRE = 0, PH_SOLVE = 1, PH_POST = 2 };
+
 struct BDesign {
   int nx, ny, P, active;       // active: OC iterations remain
   int it, max_it, R, max_cg;   // OC iterations done / requested, filter radius, PCG cap
-  int max_outer, ctas_part, pad0, pad1;
+  int max_outer, phase, pad0, pad1;  // phase: BPhase
   double e_min, pen, volfrac, move, rmin, tol;  // tol: early stop on change (0: none)
   double tol_sq, rupd2;        // PCG stop (true residual) and replacement thresholds
   // compact fields, reference numbering
@@ -49,9 +55,7 @@ struct BDesign {
   PcgCtl *ctl;
   OuterCtl *octl;
   double *part;
-  // OC bisection and compliance sum
-  OcCtl *oc;
-  double *ocpart;
+  // compliance sum
   SumCtl *sc;
   double *spart;
   double *scal;                // [0] compliance, [1..4] OC result (change, volume, lambda, steps)
@@ -86,7 +90,7 @@ __global__ void __launch_bounds__(F_THREADS)
     kb_filter(const BJob *jobs, int nj, const BDesign *ds, int which) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
-  if (!D.active) return;
+  if (!D.active || D.phase != (which ? PH_POST : PH_PRE)) return;
   const int loc = blockIdx.x - J.cta0;
   const double *x = which ? D.dc : D.rho;
   double *out = which ? D.dc_filt : D.rho_phys;
@@ -97,19 +101,29 @@ __global__ void __launch_bounds__(F_THREADS)
 __global__ void kb_scales(const BJob *jobs, int nj, const BDesign *ds) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
-  if (!D.active) return;
+  if (!D.active || D.phase != PH_PRE) return;
   scales_run(D.nx, D.ny, D.P, D.rho_phys, D.e_min, D.pen, 0.0, D.s64, D.s32, nullptr, nullptr,
              blockIdx.x - J.cta0, J.gx);
 }
 
-// one thread per slot: PCG and OC control blocks of a new OC iteration
+// one thread per slot: PCG control blocks of a new OC iteration; PRE -> SOLVE
 __global__ void kb_init(BDesign *ds, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const BDesign &D = ds[i];
-  if (!D.active) return;
+  BDesign &D = ds[i];
+  if (!D.active || D.phase != PH_PRE) return;
   ctl_init_run(D.ctl, D.tol_sq, D.rupd2, D.max_cg, D.octl, D.tol_sq, D.max_outer);
-  oc_init_run(D.oc);
+  D.phase = PH_SOLVE;
+}
+
+// one thread per slot: SOLVE -> POST once the design's solve has stopped
+__global__ void kb_mark(BDesign *ds, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BDesign &D = ds[i];
+  if (!D.active || D.phase != PH_SOLVE) return;
+  const int st = D.ctl->status;
+  if (st != TPO_SOLVE_RUNNING && st != SOLVE_NEED_UPDATE) D.phase = PH_POST;
 }
 
 template <int PRE>
@@ -192,7 +206,7 @@ __global__ void kb_cond(const BDesign *ds, int n, int *flag, unsigned *bodies,
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const BDesign &D = ds[i];
-    if (!D.active) continue;
+    if (!D.active || D.phase != PH_SOLVE) continue;
     const int st = D.ctl->status;
     if ((st == TPO_SOLVE_RUNNING || st == SOLVE_NEED_UPDATE) && D.ctl->err == 0) any = 1;
   }
@@ -210,36 +224,79 @@ __global__ void kb_cond(const BDesign *ds, int n, int *flag, unsigned *bodies,
 __global__ void kb_unpack(const BJob *jobs, int nj, const BDesign *ds) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
-  if (!D.active) return;
+  if (!D.active || D.phase != PH_POST) return;
   unpack_nodes_run(D.nx, D.ny, D.P, D.up, D.u, blockIdx.x - J.cta0, J.gx);
 }
 
 __global__ void __launch_bounds__(S_THREADS) kb_sens(const BJob *jobs, int nj, const BDesign *ds) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
-  if (!D.active) return;
+  if (!D.active || D.phase != PH_POST) return;
   const int loc = blockIdx.x - J.cta0;
   sensitivity_run(D.nx, D.ny, D.e_min, D.pen, D.rho_phys, D.u, D.dc, D.spart, D.sc, D.scal,
                   loc % J.gx, loc / J.gx, J.gx * J.gy, loc);
 }
 
-__global__ void __launch_bounds__(OC_THREADS) kb_ocstep(const BJob *jobs, int nj,
-                                                         const BDesign *ds) {
-  const BJob &J = find_job(jobs, nj);
-  const BDesign &D = ds[J.slot];
-  if (!D.active) return;
-  oc_step_run(D.nx * D.ny, D.volfrac, D.move, D.rho, D.dc_filt, nullptr, D.ocpart, D.oc,
-              blockIdx.x - J.cta0, J.gx);
-}
-
-// the design density is updated in place (each element by the thread that reads it)
-__global__ void __launch_bounds__(OC_THREADS) kb_ocfinal(const BJob *jobs, int nj,
-                                                          const BDesign *ds) {
-  const BJob &J = find_job(jobs, nj);
-  const BDesign &D = ds[J.slot];
-  if (!D.active) return;
-  oc_final_run(D.nx * D.ny, D.move, D.rho, D.dc_filt, nullptr, D.rho, D.oc, D.scal + 1,
-               blockIdx.x - J.cta0, J.gx);
+// OC update of one design per CTA (reference optimizer/oc.py:21-93, same
+// rules as k_oc_step / k_oc_final): bisection on lambda in [0, 1e9], at most
+// OC_MAX_STEPS midpoints, stop when (hi - lo) / (hi + lo) < 1e-4; the density
+// is updated in place with the last midpoint evaluated. One CTA loops over the
+// steps, so the whole bisection is one launch for every design of the batch.
+constexpr int OCB_THREADS = 1024;
+__global__ void __launch_bounds__(OCB_THREADS) kb_oc(BDesign *ds, int n) {
+  if ((int)blockIdx.x >= n) return;
+  BDesign &D = ds[blockIdx.x];
+  if (!D.active || D.phase != PH_POST) return;
+  __shared__ double red[2][OCB_THREADS / 32];
+  __shared__ double res[2];
+  const int ne = D.nx * D.ny;
+  const double *rho = D.rho;  // updated in place at the end
+  const double *__restrict__ dcf = D.dc_filt;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double lo = 0.0, hi = 1e9, lam = 0.5 * (0.0 + 1e9), last = 0.0, chg = 0.0, vol = 0.0;
+  int steps = 0;
+  for (;;) {
+    double sum = 0.0, mx = 0.0;
+    for (int e = threadIdx.x; e < ne; e += OCB_THREADS) {
+      const double r = rho[e];
+      const double nw = oc_candidate(r, dcf[e], 1.0, lam, D.move);
+      sum += nw;
+      mx = fmax(mx, fabs(nw - r));
+    }
+    sum = warp_sum(sum);
+    mx = warp_max(mx);
+    if (lane == 0) {
+      red[0][wid] = sum;
+      red[1][wid] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = red[0][0], m = red[1][0];
+      for (int w = 1; w < OCB_THREADS / 32; ++w) {
+        t += red[0][w];
+        m = fmax(m, red[1][w]);
+      }
+      res[0] = t;
+      res[1] = m;
+    }
+    __syncthreads();
+    last = lam;
+    chg = res[1];
+    vol = res[0] / ne;
+    steps += 1;
+    if (vol > D.volfrac) lo = lam; else hi = lam;
+    if ((hi - lo) / (hi + lo + 1e-30) < 1e-4 || steps >= OC_MAX_STEPS) break;
+    lam = 0.5 * (lo + hi);
+    __syncthreads();  // res[] is rewritten by the next step
+  }
+  for (int e = threadIdx.x; e < ne; e += OCB_THREADS)
+    D.rho[e] = oc_candidate(rho[e], dcf[e], 1.0, last, D.move);
+  if (threadIdx.x == 0) {
+    D.scal[1] = chg;
+    D.scal[2] = vol;
+    D.scal[3] = last;
+    D.scal[4] = (double)steps;
+  }
 }
 
 // one thread per slot: history row, iteration count, stop rule
@@ -249,7 +306,7 @@ __global__ void kb_finish(BDesign *ds, int n, int *status, int *err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   BDesign &D = ds[i];
-  if (!D.active) return;
+  if (!D.active || D.phase != PH_POST) return;
   if (D.ctl->err) atomicOr(err, 1);
   double *h = D.hist + (size_t)D.it * kBatchHist;
   h[0] = D.scal[0];
@@ -259,6 +316,7 @@ __global__ void kb_finish(BDesign *ds, int n, int *status, int *err) {
   h[4] = (double)D.octl->it;
   h[5] = (double)D.ctl->status;
   D.it += 1;
+  D.phase = PH_PRE;
   if (D.it >= D.max_it || (D.tol > 0.0 && D.it > 5 && D.scal[1] < D.tol)) D.active = 0;
   status[2 * i] = D.it;
   status[2 * i + 1] = D.active;

@@ -32,8 +32,9 @@ struct tpo_batch {
   int njobs[8]{}, nctas[8]{};
   int filter_smem = 0;
   int Ls = 16, Lu = 8;          // strip lengths (columns per CTA) of the stencil / update kinds
-  cudaGraphExec_t gexec = nullptr;
+  cudaGraphExec_t gexec = nullptr;   // OC-iteration graph
   cudaGraph_t graph = nullptr;
+  cudaGraphExec_t rexec = nullptr;   // round graph
   unsigned max_bodies = 0;
 };
 
@@ -42,7 +43,7 @@ namespace {
 using tpo::BDesign;
 using tpo::BJob;
 
-enum BKind { BK_FILTER = 0, BK_SCALES, BK_UNPACK, BK_STENCIL, BK_UPDATE, BK_SENS, BK_OC, kBK };
+enum BKind { BK_FILTER = 0, BK_SCALES, BK_UNPACK, BK_STENCIL, BK_UPDATE, BK_SENS, kBK };
 constexpr int kBatchSteps = 8;       // PCG steps per loop body (one FP64 residual check each)
 constexpr int kFlatPerThread = 4;    // elements per thread of the grid-stride kinds
 
@@ -77,12 +78,9 @@ void kind_geom(int kind, int nx, int ny, int P, int Ls, int Lu, int *gx, int *gy
       *L = Lu;
       *gy = cdiv(nx + 1, Lu);
       break;
-    case BK_SENS:
+    default:  // BK_SENS
       *gx = cdiv(ny, S_THREADS);
       *gy = cdiv(nx, SL);
-      break;
-    default:  // BK_OC
-      *gx = flat_ctas((int64_t)nx * ny, OC_THREADS);
       break;
   }
 }
@@ -105,8 +103,6 @@ struct DesignLayout {
   PcgCtl *ctl;
   OuterCtl *octl;
   double *part;
-  OcCtl *oc;
-  double *ocpart;
   SumCtl *sc;
   double *spart;
   double *scal;
@@ -137,10 +133,7 @@ DesignLayout carve_design(void *base, const tpo_batch_design *d) {
   L.ctl = cv.take<PcgCtl>(1);
   L.octl = cv.take<OuterCtl>(1);
   L.part = cv.take<double>(3 * (size_t)pcg_part_ctas(nx, ny));
-  L.oc = cv.take<OcCtl>(1);
   int gx, gy, l;
-  kind_geom(BK_OC, nx, ny, P, kMinLs, kMinLu, &gx, &gy, &l);
-  L.ocpart = cv.take<double>(2 * (size_t)gx);
   L.sc = cv.take<SumCtl>(1);
   kind_geom(BK_SENS, nx, ny, P, kMinLs, kMinLu, &gx, &gy, &l);
   L.spart = cv.take<double>((size_t)gx * gy);
@@ -214,6 +207,10 @@ int batch_rebuild(tpo_batch *b, cudaStream_t st) {
     cudaGraphDestroy(b->graph);
     b->graph = nullptr;
   }
+  if (b->rexec) {
+    cudaGraphExecDestroy(b->rexec);
+    b->rexec = nullptr;
+  }
   b->dirty = false;
   return TPO_OK;
 }
@@ -238,8 +235,10 @@ int batch_prefix(tpo_batch *b, cudaStream_t st) {
   return TPO_OK;
 }
 
+// RESX, kBatchSteps x (direction, update), then (cond >= 0) the loop test
 template <int PRE>
-int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int use_h) {
+int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int use_h,
+               bool cond = true) {
   constexpr int SMEM = StencilCfg<double, double, M_RESX, PRE>::SMEM;
   constexpr int SMEM_D = StencilCfg<float, double, M_DIR, PRE>::SMEM;
   kb_resx<PRE><<<b->nctas[BK_STENCIL], ST_THREADS, SMEM, st>>>(
@@ -253,6 +252,7 @@ int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int 
         jobs_of(b, BK_UPDATE), b->njobs[BK_UPDATE], b->d_designs);
     TPO_CK_LAUNCH();
   }
+  if (!cond) return TPO_OK;
   kb_cond<<<1, 256, 0, st>>>(b->d_designs, b->n_slots, b->d_flag, b->d_bodies, b->max_bodies, h,
                              use_h);
   TPO_CK_LAUNCH();
@@ -260,6 +260,8 @@ int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int 
 }
 
 int batch_suffix(tpo_batch *b, cudaStream_t st) {
+  kb_mark<<<cdiv(b->n_slots, 128), 128, 0, st>>>(b->d_designs, b->n_slots);
+  TPO_CK_LAUNCH();
   kb_unpack<<<b->nctas[BK_UNPACK], 256, 0, st>>>(jobs_of(b, BK_UNPACK), b->njobs[BK_UNPACK],
                                                   b->d_designs);
   TPO_CK_LAUNCH();
@@ -269,13 +271,7 @@ int batch_suffix(tpo_batch *b, cudaStream_t st) {
   kb_filter<<<b->nctas[BK_FILTER], F_THREADS, b->filter_smem, st>>>(
       jobs_of(b, BK_FILTER), b->njobs[BK_FILTER], b->d_designs, 1);
   TPO_CK_LAUNCH();
-  for (int i = 0; i < OC_MAX_STEPS; ++i) {
-    kb_ocstep<<<b->nctas[BK_OC], OC_THREADS, 0, st>>>(jobs_of(b, BK_OC), b->njobs[BK_OC],
-                                                        b->d_designs);
-    TPO_CK_LAUNCH();
-  }
-  kb_ocfinal<<<b->nctas[BK_OC], OC_THREADS, 0, st>>>(jobs_of(b, BK_OC), b->njobs[BK_OC],
-                                                       b->d_designs);
+  kb_oc<<<b->n_slots, OCB_THREADS, 0, st>>>(b->d_designs, b->n_slots);
   TPO_CK_LAUNCH();
   kb_finish<<<cdiv(b->n_slots, 128), 128, 0, st>>>(b->d_designs, b->n_slots, b->d_status,
                                                    b->d_flag + 2);
@@ -283,16 +279,23 @@ int batch_suffix(tpo_batch *b, cudaStream_t st) {
   return TPO_OK;
 }
 
-template <int PRE> int batch_body_dispatch(tpo_batch *b, cudaStream_t st,
-                                           cudaGraphConditionalHandle h, int use_h) {
-  return batch_body<PRE>(b, st, h, use_h);
-}
-int batch_body_any(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int use_h) {
+int batch_body_any(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int use_h,
+                   bool cond = true) {
   switch (b->cfg.precond) {
-    case TPO_PRECOND_NONE: return batch_body_dispatch<TPO_PRECOND_NONE>(b, st, h, use_h);
-    case TPO_PRECOND_JACOBI: return batch_body_dispatch<TPO_PRECOND_JACOBI>(b, st, h, use_h);
-    default: return batch_body_dispatch<TPO_PRECOND_NODAL_BLOCK>(b, st, h, use_h);
+    case TPO_PRECOND_NONE: return batch_body<TPO_PRECOND_NONE>(b, st, h, use_h, cond);
+    case TPO_PRECOND_JACOBI: return batch_body<TPO_PRECOND_JACOBI>(b, st, h, use_h, cond);
+    default: return batch_body<TPO_PRECOND_NODAL_BLOCK>(b, st, h, use_h, cond);
   }
+}
+
+// one round of continuous batching: PRE designs start their OC iteration,
+// every SOLVE design advances one loop body, designs whose solve stopped
+// finish their OC iteration
+int batch_round_launches(tpo_batch *b, cudaStream_t st) {
+  int rc = batch_prefix(b, st);
+  if (!rc) rc = batch_body_any(b, st, 0, 0, false);
+  if (!rc) rc = batch_suffix(b, st);
+  return rc;
 }
 
 // PCG loop driven from the host: bodies are enqueued two ahead of the flag reads
@@ -358,6 +361,22 @@ int batch_build_graph(tpo_batch *b) {
   TPO_CK(cudaStreamEndCapture(cs, &tmp));
   if (rc) return rc;
   TPO_CK(cudaGraphInstantiate(&b->gexec, g, 0));
+  return TPO_OK;
+}
+
+int batch_build_round_graph(tpo_batch *b) {
+  cudaStream_t cs = b->cap;
+  TPO_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
+  int rc = batch_round_launches(b, cs);
+  cudaGraph_t g;
+  TPO_CK(cudaStreamEndCapture(cs, &g));
+  if (rc) {
+    cudaGraphDestroy(g);
+    return rc;
+  }
+  cudaError_t e = cudaGraphInstantiate(&b->rexec, g, 0);
+  cudaGraphDestroy(g);
+  TPO_CK(e);
   return TPO_OK;
 }
 
@@ -470,6 +489,7 @@ int tpo_batch_destroy(tpo_batch *b) {
   if (!b) return TPO_OK;
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->rexec) cudaGraphExecDestroy(b->rexec);
   for (int i = 0; i < 2; ++i)
     if (b->ev[i]) cudaEventDestroy(b->ev[i]);
   if (b->cap) cudaStreamDestroy(b->cap);
@@ -541,8 +561,7 @@ int tpo_batch_add(tpo_batch *b, const tpo_batch_design *d, const double *f, cons
   D.ctl = L.ctl;
   D.octl = L.octl;
   D.part = L.part;
-  D.oc = L.oc;
-  D.ocpart = L.ocpart;
+  D.phase = PH_PRE;
   D.sc = L.sc;
   D.spart = L.spart;
   D.scal = L.scal;
@@ -597,6 +616,21 @@ int tpo_batch_oc_iteration(tpo_batch *b, tpo_stream s) {
     if ((rc = batch_prefix(b, st))) return rc;
     if ((rc = batch_pcg_host(b, st))) return rc;
     if ((rc = batch_suffix(b, st))) return rc;
+  }
+  return batch_read_status(b, st);
+}
+
+int tpo_batch_round(tpo_batch *b, tpo_stream s) {
+  if (!b) return fail(TPO_ERR_ARGS, "batch is NULL");
+  cudaStream_t st = static_cast<cudaStream_t>(s);
+  int rc;
+  if (b->dirty && (rc = batch_rebuild(b, st))) return rc;
+  if (b->nctas[BK_FILTER] == 0) return TPO_OK;
+  if (b->cfg.use_graph) {
+    if (!b->rexec && (rc = batch_build_round_graph(b))) return rc;
+    TPO_CK(cudaGraphLaunch(b->rexec, st));
+  } else if ((rc = batch_round_launches(b, st))) {
+    return rc;
   }
   return batch_read_status(b, st);
 }
