@@ -66,6 +66,17 @@ def parse_args():
     ap.add_argument("--recurrence", choices=["auto", "standard", "single"], default="auto",
                     help="PCG iteration form: one launch per iteration (auto) or the "
                          "reference's two-step recurrence (standard)")
+    ap.add_argument("--workload", choices=["bridge", "batch", "serve"], default="bridge",
+                    help="bridge: the 2048x1024 headline line; batch: uneven designs "
+                         "advanced together; serve: a Poisson request stream")
+    ap.add_argument("--designs", type=int, default=64, help="batch: number of designs")
+    ap.add_argument("--oc-iters", type=int, default=50, help="batch/serve: OC iterations")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--serial-sample", type=int, default=8,
+                    help="batch/serve: designs timed one at a time for the baseline")
+    ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
+    ap.add_argument("--rates", default="5,50,200", help="serve: arrival rates (req/s)")
+    ap.add_argument("--nelx-max", type=int, default=1024, help="serve: largest nelx")
     return ap.parse_args()
 
 
@@ -475,10 +486,114 @@ def run_case(args):
     return 0
 
 
+def run_batch(args):
+    """Uneven designs (nelx in [64, 512], aspect 1-3, MBB/cantilever/bridge,
+    seeded) advanced together, mixed precision, strip lengths from the
+    autotuner, each OC iteration one CUDA graph launch; designs/s against the
+    same designs solved one at a time (a timed sample, scaled to the batch)."""
+    import numpy as np
+    import torch
+    from toptimization_b200.batch import Batch, autotune, random_designs
+    from toptimization_b200.csrc import build as csrc_build
+    from toptimization_b200.optimizer.simp import SimpDesign
+    csrc_build.build()
+    torch.cuda.set_device(0)
+    ps = random_designs(args.designs, seed=args.seed, nelx_range=(64, 512),
+                        max_iter=args.oc_iters)
+    t = time.perf_counter()
+    tune = autotune(ps, steps=64)
+    t_tune = time.perf_counter() - t
+    out = {"metric": "designs/s (batched uneven designs, mixed, 1 GPU)",
+           "unit": "designs/s", "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+           "config": {"workload": f"{len(ps)} designs, nelx U[64,512], aspect U{{1,2,3}}, "
+                                  f"MBB/cantilever/bridge, {args.oc_iters} OC iterations, "
+                                  f"seed {args.seed}",
+                      "elements_total": int(sum(p.n_elem for p in ps)),
+                      "tiles": list(tune["best"]), "autotune_s": round(t_tune, 2),
+                      "autotune_ms": {f"{a}x{b}": round(v, 3)
+                                      for (a, b), v in tune["ms"].items()}}}
+    for mode in ("graph_oc_iterations", "rounds"):
+        b = Batch(len(ps), use_graph=True, tiles=tune["best"])
+        slots = [b.add(p) for p in ps]
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        b.run(rounds=(mode == "rounds"))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+        cg = [float(b.history(s)["cg_iters"].sum()) for s in slots]
+        out[mode] = {"seconds": round(dt, 3), "designs_per_s": round(len(ps) / dt, 4),
+                     "oc_iters_per_s": round(len(ps) * args.oc_iters / dt, 2),
+                     "cg_iters_total": int(sum(cg))}
+        b.close()
+    k = min(args.serial_sample, len(ps))
+    t = time.perf_counter()
+    for p in ps[:k]:
+        d = SimpDesign(p, precision="mixed", preconditioner=p.preconditioner)
+        for _ in range(p.max_iter):
+            d.step()
+    torch.cuda.synchronize()
+    per = (time.perf_counter() - t) / k
+    frac = sum(p.n_elem for p in ps[:k]) / sum(p.n_elem for p in ps)
+    serial_est = (time.perf_counter() - t) / frac
+    out["one_at_a_time_mixed"] = {"sample_designs": k, "seconds_per_design": round(per, 3),
+                                  "estimated_seconds_all": round(serial_est, 2),
+                                  "scaling": "sample time scaled by the element count"}
+    best = max(out["graph_oc_iterations"]["designs_per_s"], out["rounds"]["designs_per_s"])
+    out["value"] = best
+    out["speedup_vs_one_at_a_time"] = round(best * serial_est / len(ps), 2)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """Poisson request streams (seeded) served with continuous batching under a
+    150 GB HBM budget; p50/p95/p99 latency and designs/s per arrival rate,
+    beside one-at-a-time plain FP64 solves of the same requests."""
+    import torch
+    from toptimization_b200.csrc import build as csrc_build
+    from toptimization_b200.serve import Server, poisson_stream, serve_one_at_a_time
+    csrc_build.build()
+    torch.cuda.set_device(0)
+    rates = [float(r) for r in args.rates.split(",")]
+    out = {"metric": "designs/s and latency (served stream, mixed, 1 GPU)",
+           "unit": "designs/s", "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
+           "config": {"workload": f"{args.requests} requests per rate, nelx U[64,{args.nelx_max}], "
+                                  f"aspect U{{1,2,3}}, MBB/cantilever/bridge, "
+                                  f"{args.oc_iters} OC iterations, seed {args.seed}",
+                      "hbm_budget_gb": 150, "rates": rates}, "per_rate": {}}
+    for rate in rates:
+        reqs = poisson_stream(args.requests, rate, seed=args.seed,
+                              nelx_range=(64, args.nelx_max), max_iter=args.oc_iters)
+        srv = Server(hbm_budget=150e9, max_slots=256)
+        rep = srv.serve(reqs)
+        srv.close()
+        out["per_rate"][str(rate)] = rep.summary()
+    reqs = poisson_stream(args.requests, rates[-1], seed=args.seed,
+                          nelx_range=(64, args.nelx_max), max_iter=args.oc_iters)
+    k = min(args.serial_sample, len(reqs))
+    srep = serve_one_at_a_time(reqs[:k], precision="fp64")
+    ss = srep.summary()
+    out["one_at_a_time_fp64"] = dict(ss, note=f"first {k} requests of the {rates[-1]}/s stream")
+    # the batched server on exactly those requests, for a like-for-like ratio
+    srv = Server(hbm_budget=150e9, max_slots=256)
+    brep = srv.serve(reqs[:k])
+    srv.close()
+    bs = brep.summary()
+    out["batched_same_sample"] = bs
+    out["value"] = max(v["designs_per_s"] for v in out["per_rate"].values())
+    out["designs_per_s_ratio_same_sample"] = round(bs["designs_per_s"] / ss["designs_per_s"], 2)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     global _RECURRENCE
     args = parse_args()
     _RECURRENCE = args.recurrence
+    if args.workload == "batch":
+        return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     if args.case == "pcg":
         return run_case(args)
     if args.impl == "reference":

@@ -256,7 +256,7 @@ typedef struct tpo_batch_cfg {
                             node runs the PCG loop on the device); 0: host-polled loop */
   int32_t stencil_cols;  /* columns per CTA of the stencil kernels (0: default 16) */
   int32_t update_cols;   /* columns per CTA of the update kernel (0: default 8) */
-  int32_t pad;
+  int32_t round_steps;   /* PCG steps per round of tpo_batch_round (0: default 32) */
 } tpo_batch_cfg;
 
 typedef struct tpo_batch_design {
@@ -300,12 +300,13 @@ int tpo_batch_set_tiles(tpo_batch *b, int32_t stencil_cols, int32_t update_cols)
 /* One OC iteration of every active design; blocks until it is done. With
  * use_graph the iteration is one CUDA graph launch. */
 int tpo_batch_oc_iteration(tpo_batch *b, tpo_stream s);
-/* One round of continuous batching: designs about to start an OC iteration
- * start it, every design inside its PCG solve advances by one loop body
- * (one FP64 residual check and 8 PCG steps), and designs whose solve stopped
- * finish their OC iteration. Designs at different OC iterations share every
- * launch; none waits for another's solve. Blocks until done. */
-int tpo_batch_round(tpo_batch *b, tpo_stream s);
+/* `rounds` rounds of continuous batching, then one status read. In a round,
+ * designs about to start an OC iteration start it, every design inside its
+ * PCG solve advances by one loop body (one FP64 residual check and
+ * round_steps PCG steps), and designs whose solve stopped finish their OC
+ * iteration. Designs at different OC iterations share every launch; none
+ * waits for another's solve. Blocks until done. */
+int tpo_batch_round(tpo_batch *b, int32_t rounds, tpo_stream s);
 /* Per slot 0..n-1: OC iterations done (-1: empty slot) and whether more remain. */
 int tpo_batch_states(tpo_batch *b, int32_t n, int32_t *it_out, int32_t *active_out);
 /* Device time of `steps` PCG steps with the current tiles (for the autotuner;

@@ -57,7 +57,7 @@ class TpoProfile(ctypes.Structure):
 
 class TpoBatchCfg(ctypes.Structure):
     _fields_ = [("precond", c_int32), ("precision", c_int32), ("use_graph", c_int32),
-                ("stencil_cols", c_int32), ("update_cols", c_int32), ("pad", c_int32)]
+                ("stencil_cols", c_int32), ("update_cols", c_int32), ("round_steps", c_int32)]
 
 
 class TpoBatchDesign(ctypes.Structure):
@@ -118,7 +118,7 @@ _SIGS = {
     "tpo_batch_remove": (c_int, [c_void_p, c_int32]),
     "tpo_batch_set_tiles": (c_int, [c_void_p, c_int32, c_int32]),
     "tpo_batch_oc_iteration": (c_int, [c_void_p, c_void_p]),
-    "tpo_batch_round": (c_int, [c_void_p, c_void_p]),
+    "tpo_batch_round": (c_int, [c_void_p, c_int32, c_void_p]),
     "tpo_batch_states": (c_int, [c_void_p, c_int32, _PI, _PI]),
     "tpo_batch_time_steps": (c_int, [c_void_p, c_int32, c_void_p, POINTER(ctypes.c_float)]),
 }

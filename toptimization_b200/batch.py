@@ -71,7 +71,8 @@ class Batch:
     """A set of resident designs advanced together on one GPU."""
 
     def __init__(self, max_designs: int, *, preconditioner: str = "nodal_block_jacobi",
-                 use_graph: bool = True, tiles: tuple[int, int] | None = None, device=None):
+                 use_graph: bool = True, tiles: tuple[int, int] | None = None,
+                 round_steps: int = 32, device=None):
         if preconditioner not in ("jacobi", "nodal_block_jacobi", "none"):
             raise ValueError("batched designs take a point preconditioner")
         self.device = torch.device(device) if device is not None else torch.device(
@@ -85,7 +86,7 @@ class Batch:
             self.cfg = _lib.TpoBatchCfg(
                 precond=_lib.PRECOND[preconditioner], precision=_lib.PRECISION["mixed"],
                 use_graph=1 if use_graph else 0, stencil_cols=int(ls), update_cols=int(lu),
-                pad=0)
+                round_steps=int(round_steps))
             nb = self.lib.tpo_batch_workspace_bytes(int(max_designs))
             self.ws = torch.empty(nb, dtype=torch.uint8, device=self.device)
             h = ctypes.c_void_p()
@@ -134,12 +135,12 @@ class Batch:
         it, active = self.states()
         return bool(active.any())
 
-    def round(self) -> None:
-        """One round of continuous batching (`tpo_batch_round`): every design
-        advances by one PCG loop body or one OC-iteration stage, whatever the
-        OC iteration it is at."""
+    def round(self, rounds: int = 1) -> None:
+        """`rounds` rounds of continuous batching (`tpo_batch_round`), then one
+        status read: every design advances by one PCG loop body or one
+        OC-iteration stage per round, whatever the OC iteration it is at."""
         with torch.cuda.device(self.device):
-            _lib.check(self.lib.tpo_batch_round(self.handle, _lib.stream_handle()))
+            _lib.check(self.lib.tpo_batch_round(self.handle, int(rounds), _lib.stream_handle()))
 
     def states(self) -> tuple[np.ndarray, np.ndarray]:
         n = self.max_designs

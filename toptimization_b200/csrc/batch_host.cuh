@@ -32,6 +32,7 @@ struct tpo_batch {
   int njobs[8]{}, nctas[8]{};
   int filter_smem = 0;
   int Ls = 16, Lu = 8;          // strip lengths (columns per CTA) of the stencil / update kinds
+  int round_steps = 32;         // PCG steps per round
   cudaGraphExec_t gexec = nullptr;   // OC-iteration graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t rexec = nullptr;   // round graph
@@ -235,16 +236,16 @@ int batch_prefix(tpo_batch *b, cudaStream_t st) {
   return TPO_OK;
 }
 
-// RESX, kBatchSteps x (direction, update), then (cond >= 0) the loop test
+// RESX, `steps` x (direction, update), then (cond) the loop test
 template <int PRE>
 int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int use_h,
-               bool cond = true) {
+               bool cond = true, int steps = kBatchSteps) {
   constexpr int SMEM = StencilCfg<double, double, M_RESX, PRE>::SMEM;
   constexpr int SMEM_D = StencilCfg<float, double, M_DIR, PRE>::SMEM;
   kb_resx<PRE><<<b->nctas[BK_STENCIL], ST_THREADS, SMEM, st>>>(
       jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs);
   TPO_CK_LAUNCH();
-  for (int i = 0; i < kBatchSteps; ++i) {
+  for (int i = 0; i < steps; ++i) {
     kb_dir<PRE><<<b->nctas[BK_STENCIL], ST_THREADS, SMEM_D, st>>>(
         jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs);
     TPO_CK_LAUNCH();
@@ -280,11 +281,11 @@ int batch_suffix(tpo_batch *b, cudaStream_t st) {
 }
 
 int batch_body_any(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int use_h,
-                   bool cond = true) {
+                   bool cond = true, int steps = kBatchSteps) {
   switch (b->cfg.precond) {
-    case TPO_PRECOND_NONE: return batch_body<TPO_PRECOND_NONE>(b, st, h, use_h, cond);
-    case TPO_PRECOND_JACOBI: return batch_body<TPO_PRECOND_JACOBI>(b, st, h, use_h, cond);
-    default: return batch_body<TPO_PRECOND_NODAL_BLOCK>(b, st, h, use_h, cond);
+    case TPO_PRECOND_NONE: return batch_body<TPO_PRECOND_NONE>(b, st, h, use_h, cond, steps);
+    case TPO_PRECOND_JACOBI: return batch_body<TPO_PRECOND_JACOBI>(b, st, h, use_h, cond, steps);
+    default: return batch_body<TPO_PRECOND_NODAL_BLOCK>(b, st, h, use_h, cond, steps);
   }
 }
 
@@ -293,7 +294,7 @@ int batch_body_any(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, 
 // finish their OC iteration
 int batch_round_launches(tpo_batch *b, cudaStream_t st) {
   int rc = batch_prefix(b, st);
-  if (!rc) rc = batch_body_any(b, st, 0, 0, false);
+  if (!rc) rc = batch_body_any(b, st, 0, 0, false, b->round_steps);
   if (!rc) rc = batch_suffix(b, st);
   return rc;
 }
@@ -452,6 +453,7 @@ int tpo_batch_create(int32_t max_designs, const tpo_batch_cfg *cfg, void *ws, si
   b->cfg = *cfg;
   if (cfg->stencil_cols > 0) b->Ls = std::max(kMinLs, (int)cfg->stencil_cols);
   if (cfg->update_cols > 0) b->Lu = std::max(kMinLu, (int)cfg->update_cols);
+  if (cfg->round_steps > 0) b->round_steps = std::min(1024, (int)cfg->round_steps);
   Carve cv(ws);
   b->d_designs = cv.take<BDesign>((size_t)max_designs);
   b->d_jobs = cv.take<BJob>((size_t)kBK * max_designs);
@@ -620,17 +622,19 @@ int tpo_batch_oc_iteration(tpo_batch *b, tpo_stream s) {
   return batch_read_status(b, st);
 }
 
-int tpo_batch_round(tpo_batch *b, tpo_stream s) {
-  if (!b) return fail(TPO_ERR_ARGS, "batch is NULL");
+int tpo_batch_round(tpo_batch *b, int32_t rounds, tpo_stream s) {
+  if (!b || rounds < 1) return fail(TPO_ERR_ARGS, "bad arguments");
   cudaStream_t st = static_cast<cudaStream_t>(s);
   int rc;
   if (b->dirty && (rc = batch_rebuild(b, st))) return rc;
   if (b->nctas[BK_FILTER] == 0) return TPO_OK;
-  if (b->cfg.use_graph) {
-    if (!b->rexec && (rc = batch_build_round_graph(b))) return rc;
-    TPO_CK(cudaGraphLaunch(b->rexec, st));
-  } else if ((rc = batch_round_launches(b, st))) {
-    return rc;
+  for (int i = 0; i < rounds; ++i) {
+    if (b->cfg.use_graph) {
+      if (!b->rexec && (rc = batch_build_round_graph(b))) return rc;
+      TPO_CK(cudaGraphLaunch(b->rexec, st));
+    } else if ((rc = batch_round_launches(b, st))) {
+      return rc;
+    }
   }
   return batch_read_status(b, st);
 }

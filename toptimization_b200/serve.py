@@ -93,10 +93,12 @@ class Server:
 
     def __init__(self, hbm_budget: float = 150e9, max_slots: int = 256, *,
                  preconditioner: str = "nodal_block_jacobi", use_graph: bool = True,
-                 tiles: tuple[int, int] | None = None, keep_density: bool = False, device=None):
+                 tiles: tuple[int, int] | None = None, round_steps: int = 32,
+                 rounds_per_check: int = 4, keep_density: bool = False, device=None):
         self.budget = float(hbm_budget)
         self.batch = Batch(max_slots, preconditioner=preconditioner, use_graph=use_graph,
-                           tiles=tiles, device=device)
+                           tiles=tiles, round_steps=round_steps, device=device)
+        self.rounds_per_check = int(rounds_per_check)
         self.max_slots = max_slots
         self.keep_density = keep_density
 
@@ -122,8 +124,10 @@ class Server:
                 continue
             rep.peak_resident = max(rep.peak_resident, len(resident))
             rep.peak_bytes = max(rep.peak_bytes, used)
-            b.round()
-            rep.rounds += 1
+            # admission and completions are checked between groups of rounds;
+            # a request that arrives meanwhile waits at most one group
+            b.round(self.rounds_per_check)
+            rep.rounds += self.rounds_per_check
             it, act = b.states()
             t = time.perf_counter() - t0
             for slot in [s for s in resident if not act[s]]:
