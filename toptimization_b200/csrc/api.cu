@@ -480,11 +480,12 @@ LaunchBytes launch_bytes(const tpo_grid *g) {
   const int64_t nn = (int64_t)(g->nelx + 1) * (g->nely + 1), nd = 2 * nn;
   const int64_t ne = (int64_t)g->nelx * g->nely, s = sizeof(T);
   LaunchBytes lb;
+  const int64_t su = sizeof(double);  // the solution u is FP64 in both forms
   lb.dir = 4 * nd * s + ne * s + nn;  // r|z, p_old -> p, Ap; scales; mask
   if (PRE == TPO_PRECOND_BLOCK_JACOBI)
-    lb.update = 7 * nd * s + ne * s + nn;  // r, Ap, u, p -> u, r', z; weights
+    lb.update = 5 * nd * s + 2 * nd * su + ne * s + nn;  // r, Ap, p, u -> u, r', z; weights
   else
-    lb.update = 6 * nd * s + (PRE == TPO_PRECOND_NONE ? 0 : ne * s) + nn;  // u, r, p, Ap -> u, r
+    lb.update = 4 * nd * s + 2 * nd * su + (PRE == TPO_PRECOND_NONE ? 0 : ne * s) + nn;  // u, r, p, Ap -> u, r
   return lb;
 }
 
