@@ -59,8 +59,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--case", choices=["pcg"], default=None,
-                    help="profiling case: one PCG solve on the bridge, capped at --cg-iters")
+    ap.add_argument("--case", choices=["pcg", "matvec"], default=None,
+                    help="profiling case: one PCG solve on the bridge capped at --cg-iters, "
+                         "or 5 stiffness applications (FP64) on the bridge")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cg-iters", type=int, default=30)
     ap.add_argument("--recurrence", choices=["auto", "standard", "single"], default="auto",
@@ -596,6 +597,19 @@ def main():
         return run_serve(args)
     if args.case == "pcg":
         return run_case(args)
+    if args.case == "matvec":
+        import torch
+        from toptimization_b200.csrc import build as csrc_build
+        csrc_build.build()
+        torch.cuda.set_device(0)
+        from toptimization_b200 import _lib
+        from toptimization_b200.material import compute_Ke_2d, regularized_inverse
+        Ke = compute_Ke_2d(1.0, 0.3)
+        inv, alpha = regularized_inverse(Ke)
+        _lib.ensure_stiffness(Ke, inv, alpha)
+        r = time_matvec(load_workload(), torch.float64, torch, reps=5)
+        print(json.dumps({"case": "matvec", **r}))
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -220,7 +220,7 @@ template <typename T, typename C, int PRE> struct CgCfg {
       auto kern = k_cgstep<T, C, PRE, NG>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
       int o = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, ST_THREADS, SMEM) !=
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, CG_THREADS, SMEM) !=
               cudaSuccess || o < 1)
         o = 1;
       occ = o;
@@ -240,7 +240,7 @@ template <typename T, typename C, int PRE> struct CgCfg {
     dim3 grid;
     int L;
     plan(nx, ny, &grid, &L);
-    k_cgstep<T, C, PRE, NG><<<grid, ST_THREADS, SMEM, st>>>(a, L);
+    k_cgstep<T, C, PRE, NG><<<grid, CG_THREADS, SMEM, st>>>(a, L);
   }
 };
 

@@ -134,8 +134,12 @@ __device__ __forceinline__ V2<C> pre_apply(C a, C b, C d, V2<C> r) {
   return mk2<C>(fmaT(a, r.x, b * r.y), fmaT(b, r.x, d * r.y));
 }
 
+// 4 consumer warps (120 grid rows) and one producer warp that only stages
+// columns, so refills never wait for a consumer warp's arithmetic
+constexpr int CG_THREADS = (WPC + 1) * 32;
+
 template <typename T, typename C, int PRE, int NG>
-__global__ void __launch_bounds__(ST_THREADS) k_cgstep(CgArgs A, int L) {
+__global__ void __launch_bounds__(CG_THREADS) k_cgstep(CgArgs A, int L) {
   using Geo = CgGeom<T>;
   constexpr int SLOT = Geo::SLOT;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -169,8 +173,9 @@ __global__ void __launch_bounds__(ST_THREADS) k_cgstep(CgArgs A, int L) {
   const int NC = x1 - cA + 1;  // staged columns cA..x1
   const int ms = (Y0 + LEAD - 1) & ~15;
 
-  // producer (thread 0): stage column cA + k into ring slot k % NG, after the
-  // column that used the slot before (k - NG) has been released by every warp
+  // producer (lane 0 of warp WPC): stage column cA + k into ring slot k % NG,
+  // after the column that used the slot before (k - NG) has been released by
+  // every consumer warp
   auto issue = [&](int k) {
     unsigned char *sb = smem + (k % NG) * SLOT;
     uint64_t *bar = &full[k % NG];
@@ -195,12 +200,6 @@ __global__ void __launch_bounds__(ST_THREADS) k_cgstep(CgArgs A, int L) {
     if (elem_ok) bulk_g2s(sb + Geo::OFF_E, gs + (size_t)c * P + Y0 + EWin<T>::OFF, Geo::CEB, bar);
   };
   bool ok = true;
-  auto refill = [&](int k) {
-    if (k >= NC) return;
-    if (k >= NG && ok)
-      ok = mbar_wait_bounded(&empty[k % NG], ((k / NG) - 1) & 1, A.err, ERR_TMA_TIMEOUT);
-    issue(k);
-  };
   if (threadIdx.x == 0) {
     for (int i = 0; i < NG; ++i) {
       mbar_init(&full[i], 1);
@@ -209,9 +208,26 @@ __global__ void __launch_bounds__(ST_THREADS) k_cgstep(CgArgs A, int L) {
     fence_mbar_init();
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < NG - 1 && k < NC; ++k) issue(k);
-  }
+  double acc[3] = {0.0, 0.0, 0.0};  // gamma = r.u, delta = w.u, ||r||^2
+
+  if (wid == WPC) {
+    // ---- producer warp
+    if (lane == 0) {
+      int issued = 0;
+      for (int k = 0; k < NC; ++k) {
+        if (k >= NG)
+          ok = mbar_wait_bounded(&empty[k % NG], ((k / NG) - 1) & 1, A.err, ERR_TMA_TIMEOUT);
+        if (!ok) break;  // a consumer stopped releasing: issue nothing more
+        issue(k);
+        issued = k + 1;
+      }
+      if (!ok) {
+        // let the copies this CTA started land before it exits
+        for (int k = (issued > NG ? issued - NG : 0); k < issued; ++k)
+          mbar_wait_bounded(&full[k % NG], (k / NG) & 1, nullptr, 0);
+      }
+    }
+  } else {
 
   const int n_idx = y - Y0 + 2;
   const int e_idx = y - Y0 + (LEAD - 1 - EWin<T>::OFF);  // element row y-1; row y is +1
@@ -224,7 +240,6 @@ __global__ void __launch_bounds__(ST_THREADS) k_cgstep(CgArgs A, int L) {
   V2<C> un_prev = zero2, uu_prev = zero2, carry = zero2;
   C sprev_d = C(0), sprev_u = C(0);  // element column c-1, rows y-1, y
   unsigned m_prev = 0;
-  double acc[3] = {0.0, 0.0, 0.0};  // gamma = r.u, delta = w.u, ||r||^2
 
   for (int k = 0; k < NC; ++k) {
     const int c = cA + k;
@@ -287,10 +302,9 @@ __global__ void __launch_bounds__(ST_THREADS) k_cgstep(CgArgs A, int L) {
     const V2<C> tl_below = shfl_up2<C>(ftl);  // element (c-1, y-1) -> node (c-1, y)
     const V2<C> tr_below = shfl_up2<C>(ftr);  // element (c-1, y-1) -> node (c, y)
 
-    // release the column; thread 0 stages column k + NG - 1 into the slot of k - 1
+    // release the column to the producer
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[k % NG]);
-    if (threadIdx.x == 0) refill(k + NG - 1);
 
     // ---- w = K u at node (c-1, y) is complete
     const int xo = c - 1;
@@ -309,12 +323,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_cgstep(CgArgs A, int L) {
     sprev_u = scu;
     m_prev = m;
   }
-  if (!ok) {
-    // a wait ran out: let the copies this CTA started land before it exits
-    if (threadIdx.x == 0)
-      for (int k = max(0, NC - NG); k < NC; ++k)
-        mbar_wait_bounded(&full[k % NG], (k / NG) & 1, nullptr, 0);
-  }
+  }  // consumer warps
   __syncthreads();
 
   if (!grid_reduce<3>(acc, A.part, &ctl->counter)) return;
