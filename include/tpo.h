@@ -255,7 +255,7 @@ typedef struct tpo_batch_cfg {
   int32_t use_graph;     /* nonzero: each OC iteration is one CUDA graph launch (a while
                             node runs the PCG loop on the device); 0: host-polled loop */
   int32_t stencil_cols;  /* columns per CTA of the stencil kernels (0: default 16) */
-  int32_t update_cols;   /* columns per CTA of the update kernel (0: default 8) */
+  int32_t update_cols;   /* nodes per thread of the update kernel (0: default 8) */
   int32_t round_steps;   /* PCG steps per round of tpo_batch_round (0: default 32) */
 } tpo_batch_cfg;
 

@@ -178,7 +178,7 @@ template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
       auto kern = k_tstencil<T, C, MODE, PRE, G, NG>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
       int o = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, ST_THREADS, SMEM) !=
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, TS_THREADS, SMEM) !=
               cudaSuccess || o < 1)
         o = 1;
       occ = o;
@@ -199,7 +199,7 @@ template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
   }
   static int launch(cudaStream_t st, const TsArgs &a, int nx, int ny) {
     const Plan pl = plan(nx, ny);
-    k_tstencil<T, C, MODE, PRE, G, NG><<<pl.grid, ST_THREADS, SMEM, st>>>(a, pl.L);
+    k_tstencil<T, C, MODE, PRE, G, NG><<<pl.grid, TS_THREADS, SMEM, st>>>(a, pl.L);
     return TPO_OK;
   }
   static int max_ctas(int nx, int ny) {
@@ -256,6 +256,12 @@ UpdPlan update_plan(int nx, int ny) {
   strips = (nx + 1 + L - 1) / L;
   return UpdPlan{dim3(rows, strips, 1), L};
 }
+// flat update: about eight resident 256-thread CTAs per SM, grid-stride beyond
+int update_flat_ctas(int nx, int ny) {
+  const int64_t total = (int64_t)(nx + 1) * (ny + 1);
+  const int64_t want = (total + UF_THREADS - 1) / UF_THREADS;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * 8));
+}
 constexpr int kBlkL = 16;
 dim3 blk_grid(int nx, int ny) {
   const int warps_y = (ny + 1 + RPW - 1) / RPW;
@@ -272,6 +278,7 @@ int max_ctas(const tpo_grid *g) {
   // and >= 37 KB of shared memory); bound generously without querying every variant
   const int rows = (ny + 1 + RPC - 1) / RPC;
   m = std::max(m, rows * std::max(1, (nx + 1 + 7) / 8));
+  m = std::max(m, update_flat_ctas(nx, ny));
   return m;
 }
 
@@ -617,7 +624,6 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
   up.pb = w.pb;
   up.part = w.part;
   up.ctl = w.ctl;
-  const UpdPlan upl = update_plan(nx, ny);
 
   auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
@@ -628,7 +634,7 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
     if (block) {
       k_blockpre<double, double, false, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     } else {
-      k_update<double, double, PRE><<<upl.grid, UP_THREADS, 0, st>>>(up, upl.L);
+      k_update_flat<double, double, PRE><<<update_flat_ctas(nx, ny), UF_THREADS, 0, st>>>(up);
     }
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
@@ -734,7 +740,6 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   up.pb = w.fpb;
   up.part = w.part;
   up.ctl = w.ctl;
-  const UpdPlan upl = update_plan(nx, ny);
 
   auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
@@ -746,7 +751,7 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
       k_blockpre<float, double, false, kBlkL, double>
           <<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     } else {
-      k_update<float, double, PRE, double><<<upl.grid, UP_THREADS, 0, st>>>(up, upl.L);
+      k_update_flat<float, double, PRE, double><<<update_flat_ctas(nx, ny), UF_THREADS, 0, st>>>(up);
     }
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));

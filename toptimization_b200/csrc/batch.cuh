@@ -127,7 +127,7 @@ __global__ void kb_mark(BDesign *ds, int n) {
 }
 
 template <int PRE>
-__global__ void __launch_bounds__(ST_THREADS) kb_resx(const BJob *jobs, int nj, const BDesign *ds) {
+__global__ void __launch_bounds__(TS_THREADS) kb_resx(const BJob *jobs, int nj, const BDesign *ds) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
   if (!D.active) return;
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(ST_THREADS) kb_resx(const BJob *jobs, int nj, 
 }
 
 template <int PRE>
-__global__ void __launch_bounds__(ST_THREADS) kb_dir(const BJob *jobs, int nj, const BDesign *ds) {
+__global__ void __launch_bounds__(TS_THREADS) kb_dir(const BJob *jobs, int nj, const BDesign *ds) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
   if (!D.active) return;
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(ST_THREADS) kb_dir(const BJob *jobs, int nj, c
 }
 
 template <int PRE>
-__global__ void __launch_bounds__(UP_THREADS) kb_update(const BJob *jobs, int nj,
+__global__ void __launch_bounds__(UF_THREADS) kb_update(const BJob *jobs, int nj,
                                                         const BDesign *ds) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(UP_THREADS) kb_update(const BJob *jobs, int nj
   a.part = D.part;
   a.ctl = D.ctl;
   const int loc = blockIdx.x - J.cta0;
-  update_run<float, double, PRE, double>(a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy, loc);
+  update_flat_run<float, double, PRE, double>(a, loc, J.gx, J.gx, loc);
 }
 
 // Is any solve of the batch still going? flag[0] = 1 if so; flag[1] = 1 when

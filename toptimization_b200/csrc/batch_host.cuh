@@ -74,10 +74,10 @@ void kind_geom(int kind, int nx, int ny, int P, int Ls, int Lu, int *gx, int *gy
       *L = Ls;
       *gy = cdiv(nx + 1, Ls);
       break;
-    case BK_UPDATE:
-      *gx = cdiv(ny + 1, UP_THREADS);
+    case BK_UPDATE:  // flat grid-stride; Lu = nodes per thread
+      *gx = std::max(1, std::min(4096, cdiv((int64_t)(nx + 1) * (ny + 1),
+                                            (int64_t)UF_THREADS * Lu)));
       *L = Lu;
-      *gy = cdiv(nx + 1, Lu);
       break;
     default:  // BK_SENS
       *gx = cdiv(ny, S_THREADS);
@@ -242,14 +242,14 @@ int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int 
                bool cond = true, int steps = kBatchSteps) {
   constexpr int SMEM = StencilCfg<double, double, M_RESX, PRE>::SMEM;
   constexpr int SMEM_D = StencilCfg<float, double, M_DIR, PRE>::SMEM;
-  kb_resx<PRE><<<b->nctas[BK_STENCIL], ST_THREADS, SMEM, st>>>(
+  kb_resx<PRE><<<b->nctas[BK_STENCIL], TS_THREADS, SMEM, st>>>(
       jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs);
   TPO_CK_LAUNCH();
   for (int i = 0; i < steps; ++i) {
-    kb_dir<PRE><<<b->nctas[BK_STENCIL], ST_THREADS, SMEM_D, st>>>(
+    kb_dir<PRE><<<b->nctas[BK_STENCIL], TS_THREADS, SMEM_D, st>>>(
         jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs);
     TPO_CK_LAUNCH();
-    kb_update<PRE><<<b->nctas[BK_UPDATE], UP_THREADS, 0, st>>>(
+    kb_update<PRE><<<b->nctas[BK_UPDATE], UF_THREADS, 0, st>>>(
         jobs_of(b, BK_UPDATE), b->njobs[BK_UPDATE], b->d_designs);
     TPO_CK_LAUNCH();
   }

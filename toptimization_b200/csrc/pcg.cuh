@@ -22,7 +22,7 @@
 // last lane are halo rows) and walks a strip of L node columns. Column windows
 // of every input are staged into shared memory by TMA bulk copies
 // (cp.async.bulk) in groups of G columns, NG groups in flight, completion on
-// one mbarrier per ring slot; thread 0 produces, every thread consumes. Each
+// one mbarrier per ring slot; a fifth warp produces, four warps consume. Each
 // thread keeps the 3x3 neighbourhood of transformed nodal values in registers,
 // y neighbours arrive by warp shuffles. Strips overlap by two columns; values
 // there are recomputed from the inputs, never read from another strip's
@@ -36,7 +36,8 @@
 
 namespace tpo {
 
-constexpr int ST_THREADS = WPC * 32;  // 128
+constexpr int ST_THREADS = WPC * 32;  // 128 (k_blockpre)
+constexpr int TS_THREADS = ST_THREADS + 32;  // stencil: 4 consumer warps + 1 producer warp
 constexpr int UP_THREADS = 128;
 
 enum StMode { M_RAW = 0, M_DIR = 1, M_RES = 2, M_RESX = 3 };
@@ -156,13 +157,6 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     }
   };
   bool ok = true;
-  // refill slot g % NG with group g once its previous tenant (g - NG) is released
-  auto refill = [&](int g) {
-    if (g >= NGRP) return;
-    if (g >= NG && ok)
-      ok = mbar_wait_bounded(&empty[g % NG], ((g / NG) - 1) & 1, a.err, ERR_TMA_TIMEOUT);
-    issue(g);
-  };
   if (threadIdx.x == 0) {
     for (int s = 0; s < NG; ++s) {
       mbar_init(&full[s], 1);
@@ -171,9 +165,27 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     fence_mbar_init();
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int g = 0; g < NG - 1 && g < NGRP; ++g) issue(g);
-  }
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+
+  if (wid == WPC) {
+    // ---- producer warp: refill slot g % NG with group g once its previous
+    // tenant (g - NG) has been released by every consumer warp
+    if (lane == 0) {
+      int issued = 0;
+      for (int g = 0; g < NGRP; ++g) {
+        if (g >= NG)
+          ok = mbar_wait_bounded(&empty[g % NG], ((g / NG) - 1) & 1, a.err, ERR_TMA_TIMEOUT);
+        if (!ok) break;
+        issue(g);
+        issued = g + 1;
+      }
+      if (!ok)  // let the copies this CTA started land before it exits
+        for (int g = (issued > NG ? issued - NG : 0); g < issued; ++g)
+          mbar_wait_bounded(&full[g % NG], (g / NG) & 1, nullptr, 0);
+    }
+  } else {
 
   // per-lane indices inside the staged column windows
   const int n_idx = y - Y0 + 2;
@@ -189,9 +201,6 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
   C sprev_d = C(0), sprev_u = C(0);  // element column c-1, rows y-1, y
   C s2_d = C(0), s2_u = C(0);        // element column c-2, rows y-1, y (residual modes)
   unsigned m_prev = 0;
-  double acc[NV];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) acc[k] = 0.0;
 
   for (int k = 0; k < NC; ++k) {
     const int c = cA + k;
@@ -244,10 +253,9 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
 
     // this warp is done with group g: release it; thread 0 then stages
     // group g + NG - 1 into the slot of group g - 1
-    if (kk == G - 1 || k == NC - 1) {
+    if (kk == G - 1 || k == NC - 1) {  // group done: release it to the producer
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[g % NG]);
-      if (threadIdx.x == 0) refill(g + NG - 1);
     }
 
     // ---- node (xo, y), xo = c - 1, is complete
@@ -302,13 +310,8 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     m_prev = m;
   }
 
-  if (!ok) {
-    // a wait ran out: drain this CTA's copies (bounded) before its shared
-    // memory is released; the result is discarded by the host (err flag)
-    for (int g = (NGRP > NG ? NGRP - NG : 0); g < NGRP; ++g)
-      mbar_wait_bounded(&full[g % NG], (g / NG) & 1, nullptr, 0);
-  }
-  __syncthreads();  // no warp leaves while thread 0 may still be staging
+  }  // consumer warps
+  __syncthreads();  // no warp leaves while the producer may still be staging
   uint32_t *counter = (MODE == M_RESX) ? &a.octl->counter : &ctl->counter;
   if (!grid_reduce<NV>(acc, a.part, counter, nb, bid)) return;
   if (threadIdx.x != 0) return;
@@ -355,7 +358,7 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
 }
 
 template <typename T, typename C, int MODE, int PRE, int G, int NG>
-__global__ void __launch_bounds__(ST_THREADS) k_tstencil(TsArgs a, int L) {
+__global__ void __launch_bounds__(TS_THREADS) k_tstencil(TsArgs a, int L) {
   tstencil_run<T, C, MODE, PRE, G, NG>(a, L, blockIdx.x, blockIdx.y, gridDim.x * gridDim.y,
                                        blockIdx.y * gridDim.x + blockIdx.x);
 }
@@ -488,6 +491,73 @@ template <typename T, typename C, int PRE, typename X = T>
 __global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
   update_run<T, C, PRE, X>(a, L, blockIdx.x, blockIdx.y, gridDim.x * gridDim.y,
                            blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// Same update, pointwise over the grid's nodes with a flat grid-stride loop
+// (one node per thread per pass, loads coalesced along y): no column walk and
+// few registers, so enough warps are resident to keep HBM busy. The node's
+// four element scales come straight from the padded scale array: element
+// (c-1, y-1), (c-1, y), (c, y-1), (c, y) sit at the node's slot - P - 1,
+// - P, - 1 and + 0 (zero pads outside the grid rows).
+constexpr int UF_THREADS = 256;
+
+// n / d for 0 <= n < 2^31 through a double reciprocal, corrected to exact
+__device__ __forceinline__ int div_exact(int n, int d, double inv_d) {
+  int q = (int)((double)n * inv_d);
+  if ((q + 1) * d <= n) ++q;
+  if (q * d > n) --q;
+  return q;
+}
+
+template <typename T, typename C, int PRE, typename X = T>
+__device__ __forceinline__ void update_flat_run(const UpdArgs &a, int bx, int gx, int nb,
+                                                int bid) {
+  PcgCtl *ctl = a.ctl;
+  if (ctl->status != TPO_SOLVE_RUNNING) return;
+  const C alpha = C(ctl->alpha);
+  const T *__restrict__ p = static_cast<const T *>((ctl->it & 1) ? a.pa : a.pb);
+  const int nx = a.nx, ny1 = a.ny + 1, P = a.P;
+  const double inv = 1.0 / ny1;
+  const T *__restrict__ s = static_cast<const T *>(a.s);
+  X *__restrict__ u = static_cast<X *>(a.u);
+  T *__restrict__ r = static_cast<T *>(a.r);
+  const T *__restrict__ ap = static_cast<const T *>(a.ap);
+  const uint8_t *__restrict__ mask = a.mask;
+  const int total = (nx + 1) * ny1;
+  double acc[2] = {0.0, 0.0};
+  for (int n = bx * blockDim.x + threadIdx.x; n < total; n += gx * blockDim.x) {
+    const int c = div_exact(n, ny1, inv), y = n - c * ny1;
+    const size_t node = (size_t)c * P + y + LEAD;
+    const V2<X> uv = ld2<X>(u, node);
+    const V2<T> rv = ld2<T>(r, node), pv = ld2<T>(p, node), av = ld2<T>(ap, node);
+    const unsigned m = mask[node];
+    C s_ll = C(0), s_lh = C(0), s_rl = C(0), s_rh = C(0);
+    if (PRE != TPO_PRECOND_NONE) {
+      if (c >= 1) {
+        s_ll = C(s[node - P - 1]);
+        s_lh = C(s[node - P]);
+      }
+      if (c < nx) {
+        s_rl = C(s[node - 1]);
+        s_rh = C(s[node]);
+      }
+    }
+    const V2<X> un = mk2<X>(X(fmaT(alpha, C(pv.x), C(uv.x))), X(fmaT(alpha, C(pv.y), C(uv.y))));
+    const V2<T> rn = mk2<T>(T(fmaT(-alpha, C(av.x), C(rv.x))), T(fmaT(-alpha, C(av.y), C(rv.y))));
+    st2<X>(u, node, un);
+    st2<T>(r, node, rn);
+    const V2<C> rc = cvt2<C, T>(rn);
+    const V2<C> z = point_precond<C, PRE>(rc, m, s_ll, s_lh, s_rl, s_rh);
+    acc[0] += (double)rc.x * z.x + (double)rc.y * z.y;
+    acc[1] += (double)rc.x * rc.x + (double)rc.y * rc.y;
+  }
+  if (!grid_reduce<2>(acc, a.part, &ctl->counter, nb, bid)) return;
+  if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
+}
+
+template <typename T, typename C, int PRE, typename X = T>
+__global__ void __launch_bounds__(UF_THREADS) k_update_flat(UpdArgs a) {
+  update_flat_run<T, C, PRE, X>(a, blockIdx.x, gridDim.x, gridDim.x, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
