@@ -339,7 +339,7 @@ PcgWs carve_pcg(void *base, const tpo_grid *g, const tpo_solve_cfg *c) {
     w.fpa = cv.take<float>(2 * NN);
     w.fpb = cv.take<float>(2 * NN);
     w.fap = cv.take<float>(2 * NN);
-    if (block) w.fz = cv.take<float>(2 * NN);
+    w.fz = cv.take<float>(2 * NN);  // z (the element-block z, or M r stored by the update)
   } else {
     if (block) w.w64 = cv.take<double>(NE);
     w.ra = cv.take<double>(2 * NN);
@@ -347,7 +347,7 @@ PcgWs carve_pcg(void *base, const tpo_grid *g, const tpo_solve_cfg *c) {
     w.pa = cv.take<double>(2 * NN);
     w.pb = cv.take<double>(2 * NN);
     w.ap = cv.take<double>(2 * NN);
-    if (block) w.z = cv.take<double>(2 * NN);
+    w.z = cv.take<double>(2 * NN);
   }
   w.bytes = cv.off;
   return w;
@@ -491,8 +491,8 @@ LaunchBytes launch_bytes(const tpo_grid *g) {
   lb.dir = 4 * nd * s + ne * s + nn;  // r|z, p_old -> p, Ap; scales; mask
   if (PRE == TPO_PRECOND_BLOCK_JACOBI)
     lb.update = 5 * nd * s + 2 * nd * su + ne * s + nn;  // r, Ap, p, u -> u, r', z; weights
-  else
-    lb.update = 4 * nd * s + 2 * nd * su + (PRE == TPO_PRECOND_NONE ? 0 : ne * s) + nn;  // u, r, p, Ap -> u, r
+  else  // u, r, p, Ap -> u, r, z
+    lb.update = 5 * nd * s + 2 * nd * su + (PRE == TPO_PRECOND_NONE ? 0 : ne * s) + nn;
   return lb;
 }
 
@@ -596,6 +596,10 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
   if (block) {
     k_blockpre<double, double, true, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     TPO_CK_LAUNCH();
+  } else {
+    k_precond_flat<double, double, PRE><<<update_flat_ctas(nx, ny), UF_THREADS, 0, st>>>(
+        nx, ny, P, w.s64, w.mask, w.ra, w.z);
+    TPO_CK_LAUNCH();
   }
 
   TsArgs d{};
@@ -604,7 +608,7 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
   d.P = P;
   d.s = w.s64;
   d.mask = w.mask;
-  d.a = block ? (const void *)w.z : (const void *)w.ra;
+  d.a = w.z;  // z from the update kernel (or the element-block preconditioner)
   d.pa = w.pa;
   d.pb = w.pb;
   d.out = w.ap;
@@ -624,10 +628,11 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
   up.pb = w.pb;
   up.part = w.part;
   up.ctl = w.ctl;
+  up.z = w.z;
 
   auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
-    StencilCfg<double, double, M_DIR, PRE>::launch(st, d, nx, ny);
+    StencilCfg<double, double, M_DIR, TPO_PRECOND_BLOCK_JACOBI>::launch(st, d, nx, ny);  // reads z
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
@@ -720,7 +725,7 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   d.P = P;
   d.s = w.s32;
   d.mask = w.mask;
-  d.a = block ? (const void *)w.fz : (const void *)w.fra;
+  d.a = w.fz;  // z from the update kernel (or the element-block preconditioner)
   d.pa = w.fpa;
   d.pb = w.fpb;
   d.out = w.fap;
@@ -740,10 +745,11 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
   up.pb = w.fpb;
   up.part = w.part;
   up.ctl = w.ctl;
+  up.z = w.fz;
 
   auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
-    StencilCfg<float, double, M_DIR, PRE>::launch(st, d, nx, ny);
+    StencilCfg<float, double, M_DIR, TPO_PRECOND_BLOCK_JACOBI>::launch(st, d, nx, ny);  // reads z
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
@@ -772,6 +778,10 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
     if (block) {
       k_blockpre<float, double, true, kBlkL, double>
           <<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
+      TPO_CK_LAUNCH();
+    } else {  // z of the replaced residual (no-op when the replacement did not run)
+      k_precond_flat<float, double, PRE><<<update_flat_ctas(nx, ny), UF_THREADS, 0, st>>>(
+          nx, ny, P, w.s32, w.mask, w.fra, w.fz);
       TPO_CK_LAUNCH();
     }
     TPO_CK(cudaMemcpyAsync(&oh, w.octl, sizeof(OuterCtl), cudaMemcpyDeviceToHost, st));

@@ -378,6 +378,7 @@ struct UpdArgs {
   const void *pa, *pb;
   double *part;
   PcgCtl *ctl;
+  void *z;  // flat update: optional output z = M r (T), read by the next direction kernel
 };
 
 __device__ __forceinline__ void finish_update(PcgCtl *ctl, double rz_new, double rr) {
@@ -547,12 +548,53 @@ __device__ __forceinline__ void update_flat_run(const UpdArgs &a, int bx, int gx
     st2<X>(u, node, un);
     st2<T>(r, node, rn);
     const V2<C> rc = cvt2<C, T>(rn);
-    const V2<C> z = point_precond<C, PRE>(rc, m, s_ll, s_lh, s_rl, s_rh);
+    V2<C> z = point_precond<C, PRE>(rc, m, s_ll, s_lh, s_rl, s_rh);
+    if (a.z) {  // r.z with the stored (rounded) z, the one the direction update uses
+      const V2<T> zt = mk2<T>(T(z.x), T(z.y));
+      st2<T>(static_cast<T *>(a.z), node, zt);
+      z = cvt2<C, T>(zt);
+    }
     acc[0] += (double)rc.x * z.x + (double)rc.y * z.y;
     acc[1] += (double)rc.x * rc.x + (double)rc.y * rc.y;
   }
   if (!grid_reduce<2>(acc, a.part, &ctl->counter, nb, bid)) return;
   if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
+}
+
+// z = M r over the grid's nodes (flat), after an FP64 residual replacement:
+// the direction kernel reads z instead of recomputing it
+template <typename T, typename C, int PRE>
+__device__ __forceinline__ void precond_flat_run(int nx, int ny, int P, const T *__restrict__ s,
+                                                 const uint8_t *__restrict__ mask,
+                                                 const T *__restrict__ r, T *__restrict__ z,
+                                                 int bx, int gx) {
+  const int ny1 = ny + 1;
+  const double inv = 1.0 / ny1;
+  const int total = (nx + 1) * ny1;
+  for (int n = bx * blockDim.x + threadIdx.x; n < total; n += gx * blockDim.x) {
+    const int c = div_exact(n, ny1, inv), y = n - c * ny1;
+    const size_t node = (size_t)c * P + y + LEAD;
+    C s_ll = C(0), s_lh = C(0), s_rl = C(0), s_rh = C(0);
+    if (PRE != TPO_PRECOND_NONE) {
+      if (c >= 1) {
+        s_ll = C(s[node - P - 1]);
+        s_lh = C(s[node - P]);
+      }
+      if (c < nx) {
+        s_rl = C(s[node - 1]);
+        s_rh = C(s[node]);
+      }
+    }
+    const V2<C> zz = point_precond<C, PRE>(cvt2<C, T>(ld2<T>(r, node)), mask[node], s_ll, s_lh,
+                                           s_rl, s_rh);
+    st2<T>(z, node, mk2<T>(T(zz.x), T(zz.y)));
+  }
+}
+template <typename T, typename C, int PRE>
+__global__ void __launch_bounds__(UF_THREADS) k_precond_flat(int nx, int ny, int P, const T *s,
+                                                             const uint8_t *mask, const T *r,
+                                                             T *z) {
+  precond_flat_run<T, C, PRE>(nx, ny, P, s, mask, r, z, blockIdx.x, gridDim.x);
 }
 
 template <typename T, typename C, int PRE, typename X = T>
