@@ -94,12 +94,15 @@ def test_autotune_reports_every_candidate(tpo_built):
     res = autotune(ps, candidates=[(8, 4), (16, 8), (32, 16)], steps=16)
     assert set(res["ms"]) == {(8, 4), (16, 8), (32, 16)}
     assert res["best"] in res["ms"] and all(v > 0 for v in res["ms"].values())
-    # results do not depend on the tiles beyond rounding order: same convergence
+    # other tiles change the rounding order of the FP32 Krylov vectors, so the
+    # two solves take different paths; both meet the FP64 stop rule
+    # ||f - K u|| < 1e-8 ||f||, which bounds the compliance gap by about
+    # ||r|| ||K^-1 f|| / c, a few 1e-7 on these designs
     a = _run(ps[:2], tiles=(8, 4))
     c = _run(ps[:2], tiles=(32, 16))
     for i in range(2):
         ca, cc = a[i][1]["compliance"], c[i][1]["compliance"]
-        assert abs(ca[0] - cc[0]) / ca[0] < 1e-7
+        assert abs(ca[0] - cc[0]) / ca[0] < 1e-6
 
 
 def test_rounds_and_oc_iterations_agree(tpo_built):

@@ -51,7 +51,7 @@ struct BDesign {
   // padded PCG state of the mixed form
   uint8_t *mask;
   double *up, *fp, *s64;
-  float *s32, *fr, *fpa, *fpb, *fap;
+  float *s32, *fr, *fpa, *fpb, *fap, *fz;  // fz = M r, written by the update kernel
   PcgCtl *ctl;
   OuterCtl *octl;
   double *part;
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(TS_THREADS) kb_dir(const BJob *jobs, int nj, c
   a.P = D.P;
   a.s = D.s32;
   a.mask = D.mask;
-  a.a = D.fr;
+  a.a = D.fz;  // z = M r from the update kernel (or the pass after a replacement)
   a.pa = D.fpa;
   a.pb = D.fpb;
   a.out = D.fap;
@@ -169,8 +169,19 @@ __global__ void __launch_bounds__(TS_THREADS) kb_dir(const BJob *jobs, int nj, c
   a.ctl = D.ctl;
   a.err = &D.ctl->err;
   const int loc = blockIdx.x - J.cta0;
-  tstencil_run<float, double, M_DIR, PRE, 2, 4>(a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy,
-                                                loc);
+  tstencil_run<float, double, M_DIR, TPO_PRECOND_BLOCK_JACOBI, 2, 4>(
+      a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy, loc);
+}
+
+// z = M r for every design in its solve (after the FP64 residual replacement
+// of a loop body; for the others it rewrites the z their update stored)
+template <int PRE>
+__global__ void __launch_bounds__(UF_THREADS) kb_pre(const BJob *jobs, int nj, const BDesign *ds) {
+  const BJob &J = find_job(jobs, nj);
+  const BDesign &D = ds[J.slot];
+  if (!D.active || D.phase != PH_SOLVE || D.ctl->status != TPO_SOLVE_RUNNING) return;
+  precond_flat_run<float, double, PRE>(D.nx, D.ny, D.P, D.s32, D.mask, D.fr, D.fz,
+                                       blockIdx.x - J.cta0, J.gx);
 }
 
 template <int PRE>
@@ -192,6 +203,7 @@ __global__ void __launch_bounds__(UF_THREADS) kb_update(const BJob *jobs, int nj
   a.pb = D.fpb;
   a.part = D.part;
   a.ctl = D.ctl;
+  a.z = D.fz;
   const int loc = blockIdx.x - J.cta0;
   update_flat_run<float, double, PRE, double>(a, loc, J.gx, J.gx, loc);
 }

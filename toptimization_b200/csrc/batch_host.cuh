@@ -100,7 +100,7 @@ struct DesignLayout {
   double *rho, *rho_phys, *dc, *dc_filt, *u, *hist;
   uint8_t *mask;
   double *up, *fp, *s64;
-  float *s32, *fr, *fpa, *fpb, *fap;
+  float *s32, *fr, *fpa, *fpb, *fap, *fz;
   PcgCtl *ctl;
   OuterCtl *octl;
   double *part;
@@ -131,6 +131,7 @@ DesignLayout carve_design(void *base, const tpo_batch_design *d) {
   L.fpa = cv.take<float>(2 * NN);
   L.fpb = cv.take<float>(2 * NN);
   L.fap = cv.take<float>(2 * NN);
+  L.fz = cv.take<float>(2 * NN);
   L.ctl = cv.take<PcgCtl>(1);
   L.octl = cv.take<OuterCtl>(1);
   L.part = cv.take<double>(3 * (size_t)pcg_part_ctas(nx, ny));
@@ -244,6 +245,9 @@ int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int 
   constexpr int SMEM_D = StencilCfg<float, double, M_DIR, PRE>::SMEM;
   kb_resx<PRE><<<b->nctas[BK_STENCIL], TS_THREADS, SMEM, st>>>(
       jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs);
+  TPO_CK_LAUNCH();
+  kb_pre<PRE><<<b->nctas[BK_UPDATE], UF_THREADS, 0, st>>>(jobs_of(b, BK_UPDATE),
+                                                            b->njobs[BK_UPDATE], b->d_designs);
   TPO_CK_LAUNCH();
   for (int i = 0; i < steps; ++i) {
     kb_dir<PRE><<<b->nctas[BK_STENCIL], TS_THREADS, SMEM_D, st>>>(
@@ -560,6 +564,7 @@ int tpo_batch_add(tpo_batch *b, const tpo_batch_design *d, const double *f, cons
   D.fpa = L.fpa;
   D.fpb = L.fpb;
   D.fap = L.fap;
+  D.fz = L.fz;
   D.ctl = L.ctl;
   D.octl = L.octl;
   D.part = L.part;
