@@ -133,14 +133,18 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned by
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+// One poll of a phase. A thread whose phase is not complete is suspended until
+// it completes or kSuspendNs elapse, so waiting warps do not spin through
+// issue slots that the other warps of the SM need.
+constexpr unsigned kSuspendNs = 20000;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
   unsigned ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
@@ -155,11 +159,11 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 }
 
 // Bounded wait on an mbarrier phase. Returns false (and records the failure
-// in *err) if the phase has not completed after `limit` polls; try_wait
-// itself suspends the thread for a while on each poll.
+// in *err) if the phase has not completed after kLimit polls of at most
+// kSuspendNs each (about 1.3 s in all).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int *err,
                                                   int code) {
-  constexpr int kLimit = 1 << 20;
+  constexpr int kLimit = 1 << 16;
   for (int i = 0; i < kLimit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   if (err) atomicExch(err, code);
