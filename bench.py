@@ -412,8 +412,8 @@ def run_ours(args):
     # dominant PCG kernel of the timed (mixed) step, by device time in the timing pass
     km = kern_mixed
     key = max(km, key=lambda k: km[k]["total_ms"])
-    names = {"dir": "k_tstencil<float,double,DIR,nodal> (direction + matvec, TMA-staged)",
-             "update": "k_update<float,double,nodal> (update + preconditioner)",
+    names = {"dir": "k_tstencil<float,double,DIR> (p = z + beta p, K p, p.Kp; TMA-staged)",
+             "update": "k_update_flat<float,double,nodal,double> (u, r update, z = M r, r.z)",
              "step": "k_cgstep<float,double,nodal> (whole PCG iteration in one launch, "
                      "TMA-staged)"}
     kd = km[key]
