@@ -303,41 +303,29 @@ def run_reference(args):
 def run_ours(args):
     import numpy as np
     import torch
-    import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from toptimization_b200 import replicas
+    rk = replicas.from_env()
+    world, rank, local = rk.world, rk.rank, rk.local
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+    replicas.init(rk, "nccl", 300, torch.device("cuda", local))
 
     from toptimization_b200 import _lib
     from toptimization_b200.csrc import build as csrc_build
     from toptimization_b200.optimizer.simp import SimpDesign, run
     if rank == 0:
         csrc_build.build()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(rk)  # the library is built once, by rank 0
     lib = _lib.load()
     dev = torch.device("cuda", local)
     pr = load_workload()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
     def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replicas.barrier(rk)
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, rk, dev)
 
     # ---- mixed (headline), timed
     mixed = SimpDesign(pr, device=dev, precision="mixed", preconditioner=PRECONDITIONER)
@@ -403,8 +391,7 @@ def run_ours(args):
                         "per-iteration D2H of the density to a viz_callback and of 5 scalars)")}
 
     if rank != 0:
-        if world > 1:
-            dist.destroy_process_group()
+        replicas.finish(rk)
         return 0
 
     value = world * args.steps / (t_mixed / 1e3)
@@ -450,8 +437,7 @@ def run_ours(args):
         cg = int(round(fp64["cg_iters_mean"])) if fp64 else FP64_CG_PER_OC
         line["cpu_baseline"] = cpu_sample(pr, cg)
     print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish(rk)
     return 0
 
 
@@ -497,10 +483,16 @@ def run_batch(args):
     from toptimization_b200.batch import Batch, autotune, random_designs
     from toptimization_b200.csrc import build as csrc_build
     from toptimization_b200.optimizer.simp import SimpDesign
-    csrc_build.build()
-    torch.cuda.set_device(0)
-    ps = random_designs(args.designs, seed=args.seed, nelx_range=(64, 512),
-                        max_iter=args.oc_iters)
+    from toptimization_b200 import replicas
+    rk = replicas.from_env()
+    torch.cuda.set_device(rk.local)
+    replicas.init(rk, "nccl", 600, torch.device("cuda", rk.local))
+    if rk.rank == 0:
+        csrc_build.build()
+    replicas.barrier(rk)
+    # every rank draws the same designs and runs its round-robin share
+    ps = replicas.shard(random_designs(args.designs, seed=args.seed, nelx_range=(64, 512),
+                                       max_iter=args.oc_iters), rk)
     t = time.perf_counter()
     tune = autotune(ps, steps=64)
     t_tune = time.perf_counter() - t
@@ -516,16 +508,21 @@ def run_batch(args):
     for mode in ("graph_oc_iterations", "rounds"):
         b = Batch(len(ps), use_graph=True, tiles=tune["best"])
         slots = [b.add(p) for p in ps]
-        torch.cuda.synchronize()
+        replicas.barrier(rk)
         t = time.perf_counter()
         b.run(rounds=(mode == "rounds"))
-        torch.cuda.synchronize()
-        dt = time.perf_counter() - t
+        replicas.barrier(rk)
+        dt = replicas.max_over_ranks(time.perf_counter() - t, rk,
+                                     torch.device("cuda", rk.local))
         cg = [float(b.history(s)["cg_iters"].sum()) for s in slots]
-        out[mode] = {"seconds": round(dt, 3), "designs_per_s": round(len(ps) / dt, 4),
-                     "oc_iters_per_s": round(len(ps) * args.oc_iters / dt, 2),
-                     "cg_iters_total": int(sum(cg))}
+        out[mode] = {"seconds": round(dt, 3),
+                     "designs_per_s": round(replicas.job_rate(len(ps), dt, rk), 4),
+                     "oc_iters_per_s": round(replicas.job_rate(len(ps) * args.oc_iters, dt, rk),
+                                             2),
+                     "cg_iters_total_rank0": int(sum(cg))}
         b.close()
+    out["n_gpus"] = rk.world
+    out["scaling"] = "weak" if rk.multi else None
     k = min(args.serial_sample, len(ps))
     t = time.perf_counter()
     for p in ps[:k]:
@@ -541,8 +538,10 @@ def run_batch(args):
                                   "scaling": "sample time scaled by the element count"}
     best = max(out["graph_oc_iterations"]["designs_per_s"], out["rounds"]["designs_per_s"])
     out["value"] = best
-    out["speedup_vs_one_at_a_time"] = round(best * serial_est / len(ps), 2)
-    print(json.dumps(out), flush=True)
+    out["speedup_vs_one_at_a_time"] = round(best / rk.world * serial_est / len(ps), 2)
+    if rk.rank == 0:
+        print(json.dumps(out), flush=True)
+    replicas.finish(rk)
     return 0
 
 
@@ -553,9 +552,38 @@ def run_serve(args):
     import torch
     from toptimization_b200.csrc import build as csrc_build
     from toptimization_b200.serve import Server, poisson_stream, serve_one_at_a_time
-    csrc_build.build()
-    torch.cuda.set_device(0)
+    import torch.distributed as dist
+    from toptimization_b200 import replicas
+    from toptimization_b200.serve import ServeReport
+    rk = replicas.from_env()
+    torch.cuda.set_device(rk.local)
+    replicas.init(rk, "nccl", 1800, torch.device("cuda", rk.local))
+    if rk.rank == 0:
+        csrc_build.build()
+    replicas.barrier(rk)
     rates = [float(r) for r in args.rates.split(",")]
+
+    def served(reqs, server):
+        """Each rank serves its round-robin share; completions of all ranks are
+        gathered so the latency percentiles cover the whole stream."""
+        rep = server(replicas.shard(reqs, rk))
+        if rk.multi:
+            parts = [None] * rk.world
+            dist.all_gather_object(parts, [(c.rid, c.arrival, c.admitted, c.done, c.oc_iters,
+                                            c.compliance) for c in rep.completions])
+            from toptimization_b200.serve import Completion
+            allc = [Completion(*t) for part in parts for t in part]
+            rep = ServeReport(sorted(allc, key=lambda c: c.rid), rep.rounds, rep.peak_resident,
+                              rep.peak_bytes, rep.wall)
+        return rep
+
+    def batched(reqs):
+        srv = Server(hbm_budget=150e9, max_slots=256)
+        try:
+            return srv.serve(reqs)
+        finally:
+            srv.close()
+
     out = {"metric": "designs/s and latency (served stream, mixed, 1 GPU)",
            "unit": "designs/s", "higher_is_better": True, "n_gpus": 1, "data": "synthetic",
            "config": {"workload": f"{args.requests} requests per rate, nelx U[64,{args.nelx_max}], "
@@ -565,25 +593,21 @@ def run_serve(args):
     for rate in rates:
         reqs = poisson_stream(args.requests, rate, seed=args.seed,
                               nelx_range=(64, args.nelx_max), max_iter=args.oc_iters)
-        srv = Server(hbm_budget=150e9, max_slots=256)
-        rep = srv.serve(reqs)
-        srv.close()
-        out["per_rate"][str(rate)] = rep.summary()
+        out["per_rate"][str(rate)] = served(reqs, batched).summary()
     reqs = poisson_stream(args.requests, rates[-1], seed=args.seed,
                           nelx_range=(64, args.nelx_max), max_iter=args.oc_iters)
     k = min(args.serial_sample, len(reqs))
-    srep = serve_one_at_a_time(reqs[:k], precision="fp64")
-    ss = srep.summary()
+    ss = served(reqs[:k], lambda r: serve_one_at_a_time(r, precision="fp64")).summary()
     out["one_at_a_time_fp64"] = dict(ss, note=f"first {k} requests of the {rates[-1]}/s stream")
     # the batched server on exactly those requests, for a like-for-like ratio
-    srv = Server(hbm_budget=150e9, max_slots=256)
-    brep = srv.serve(reqs[:k])
-    srv.close()
-    bs = brep.summary()
+    bs = served(reqs[:k], batched).summary()
     out["batched_same_sample"] = bs
     out["value"] = max(v["designs_per_s"] for v in out["per_rate"].values())
     out["designs_per_s_ratio_same_sample"] = round(bs["designs_per_s"] / ss["designs_per_s"], 2)
-    print(json.dumps(out), flush=True)
+    out["n_gpus"] = rk.world
+    if rk.rank == 0:
+        print(json.dumps(out), flush=True)
+    replicas.finish(rk)
     return 0
 
 
