@@ -522,40 +522,64 @@ __device__ __forceinline__ void update_flat_run(const UpdArgs &a, int bx, int gx
   const T *__restrict__ s = static_cast<const T *>(a.s);
   X *__restrict__ u = static_cast<X *>(a.u);
   T *__restrict__ r = static_cast<T *>(a.r);
+  T *__restrict__ zo = static_cast<T *>(a.z);
   const T *__restrict__ ap = static_cast<const T *>(a.ap);
   const uint8_t *__restrict__ mask = a.mask;
   const int total = (nx + 1) * ny1;
-  double acc[2] = {0.0, 0.0};
-  for (int n = bx * blockDim.x + threadIdx.x; n < total; n += gx * blockDim.x) {
+  struct Node {
+    size_t slot;
+    V2<X> u;
+    V2<T> r, p, ap;
+    C s_ll, s_lh, s_rl, s_rh;
+    unsigned m;
+    bool ok;
+  };
+  auto load = [&](int n, Node &d) {
+    d.ok = n < total;
+    if (!d.ok) return;
     const int c = div_exact(n, ny1, inv), y = n - c * ny1;
-    const size_t node = (size_t)c * P + y + LEAD;
-    const V2<X> uv = ld2<X>(u, node);
-    const V2<T> rv = ld2<T>(r, node), pv = ld2<T>(p, node), av = ld2<T>(ap, node);
-    const unsigned m = mask[node];
-    C s_ll = C(0), s_lh = C(0), s_rl = C(0), s_rh = C(0);
+    d.slot = (size_t)c * P + y + LEAD;
+    d.u = ld2<X>(u, d.slot);
+    d.r = ld2<T>(r, d.slot);
+    d.p = ld2<T>(p, d.slot);
+    d.ap = ld2<T>(ap, d.slot);
+    d.m = mask[d.slot];
+    d.s_ll = d.s_lh = d.s_rl = d.s_rh = C(0);
     if (PRE != TPO_PRECOND_NONE) {
       if (c >= 1) {
-        s_ll = C(s[node - P - 1]);
-        s_lh = C(s[node - P]);
+        d.s_ll = C(s[d.slot - P - 1]);
+        d.s_lh = C(s[d.slot - P]);
       }
       if (c < nx) {
-        s_rl = C(s[node - 1]);
-        s_rh = C(s[node]);
+        d.s_rl = C(s[d.slot - 1]);
+        d.s_rh = C(s[d.slot]);
       }
     }
-    const V2<X> un = mk2<X>(X(fmaT(alpha, C(pv.x), C(uv.x))), X(fmaT(alpha, C(pv.y), C(uv.y))));
-    const V2<T> rn = mk2<T>(T(fmaT(-alpha, C(av.x), C(rv.x))), T(fmaT(-alpha, C(av.y), C(rv.y))));
-    st2<X>(u, node, un);
-    st2<T>(r, node, rn);
+  };
+  double acc[2] = {0.0, 0.0};
+  auto update = [&](const Node &d) {
+    if (!d.ok) return;
+    const V2<X> un = mk2<X>(X(fmaT(alpha, C(d.p.x), C(d.u.x))), X(fmaT(alpha, C(d.p.y), C(d.u.y))));
+    const V2<T> rn = mk2<T>(T(fmaT(-alpha, C(d.ap.x), C(d.r.x))),
+                            T(fmaT(-alpha, C(d.ap.y), C(d.r.y))));
+    st2<X>(u, d.slot, un);
+    st2<T>(r, d.slot, rn);
     const V2<C> rc = cvt2<C, T>(rn);
-    V2<C> z = point_precond<C, PRE>(rc, m, s_ll, s_lh, s_rl, s_rh);
-    if (a.z) {  // r.z with the stored (rounded) z, the one the direction update uses
+    C pa, pb, pd;
+    node_pre<C, PRE>(d.m, d.s_ll, d.s_lh, d.s_rl, d.s_rh, pa, pb, pd);
+    V2<C> z = pre_apply<C>(pa, pb, pd, rc);
+    if (zo) {  // r.z with the stored (rounded) z, the one the direction update uses
       const V2<T> zt = mk2<T>(T(z.x), T(z.y));
-      st2<T>(static_cast<T *>(a.z), node, zt);
+      st2<T>(zo, d.slot, zt);
       z = cvt2<C, T>(zt);
     }
     acc[0] += (double)rc.x * z.x + (double)rc.y * z.y;
     acc[1] += (double)rc.x * rc.x + (double)rc.y * rc.y;
+  };
+  for (int n = bx * blockDim.x + threadIdx.x; n < total; n += gx * blockDim.x) {
+    Node d;
+    load(n, d);
+    update(d);
   }
   if (!grid_reduce<2>(acc, a.part, &ctl->counter, nb, bid)) return;
   if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
@@ -585,8 +609,9 @@ __device__ __forceinline__ void precond_flat_run(int nx, int ny, int P, const T 
         s_rh = C(s[node]);
       }
     }
-    const V2<C> zz = point_precond<C, PRE>(cvt2<C, T>(ld2<T>(r, node)), mask[node], s_ll, s_lh,
-                                           s_rl, s_rh);
+    C pa, pb, pd;
+    node_pre<C, PRE>(mask[node], s_ll, s_lh, s_rl, s_rh, pa, pb, pd);
+    const V2<C> zz = pre_apply<C>(pa, pb, pd, cvt2<C, T>(ld2<T>(r, node)));
     st2<T>(z, node, mk2<T>(T(zz.x), T(zz.y)));
   }
 }

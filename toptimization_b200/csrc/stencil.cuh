@@ -120,6 +120,78 @@ __device__ __forceinline__ V2<T> point_precond(V2<T> r, unsigned m, T s_ll, T s_
   }
 }
 
+// 1/x for x inside FP32's normal range: the approximate FP32 reciprocal
+// (rcp.approx, relative error below 2^-22) as the seed, then two Newton-Raphson
+// steps y <- y + y (1 - x y) in FP64, each of which squares the relative error
+// (2^-22 -> 2^-44 -> below FP64 rounding).
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y = (double)rcp_approx((float)x);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+// z = [[a, b], [b, d]] r: the point preconditioner of node (x, y) from its
+// four element scales (s_ll = (x-1,y-1), s_lh = (x-1,y), s_rl = (x,y-1),
+// s_rh = (x,y)). Same operator as point_precond (stencil.cuh), written for
+// the square-Q4 Ke: every diagonal entry is K00, and the x-y entry of
+// corner a's block is +K01, -K01, +K01, -K01 for a = 0..3.
+//  JACOBI: diag = K00 sum(s) (fixed DOF -> 1, floor 1e-20), reference
+//          fem/kernels.py:65-101.
+//  NODAL:  B = [[K00 S, K01 D], [K01 D, K00 S]], S = sum(s),
+//          D = s_ll - s_lh - s_rl + s_rh (the corner signs), fixed DOFs get an
+//          identity row and column; a singular block falls back to Jacobi.
+template <typename C, int PRE>
+__device__ __forceinline__ void node_pre(unsigned m, C s_ll, C s_lh, C s_rl, C s_rh, C &a, C &b,
+                                         C &d) {
+  if constexpr (PRE == TPO_PRECOND_NONE) {
+    a = d = C(1);
+    b = C(0);
+  } else {
+    const C k00 = kst<C>(4);
+    const C S = (s_ll + s_lh) + (s_rl + s_rh);
+    C bxx = k00 * S, byy = bxx;
+    if constexpr (PRE == TPO_PRECOND_JACOBI) {
+      if (m & FIXED_X) bxx = C(1); else if (bxx < C(1e-20)) bxx = C(1e-20);
+      if (m & FIXED_Y) byy = C(1); else if (byy < C(1e-20)) byy = C(1e-20);
+      a = rcp_nr(bxx);
+      d = (byy == bxx) ? a : rcp_nr(byy);
+      b = C(0);
+    } else {
+      C bxy = kst<C>(5) * ((s_ll - s_lh) + (s_rh - s_rl));
+      if (m & FIXED_X) { bxx = C(1); bxy = C(0); }
+      if (m & FIXED_Y) { byy = C(1); bxy = C(0); }
+      const C det = bxx * byy - bxy * bxy;
+      if (det > C(1e-36)) {
+        const C inv = rcp_nr(det);
+        a = byy * inv;
+        d = bxx * inv;
+        b = -bxy * inv;
+      } else if (det > C(0)) {
+        const C inv = C(1) / det;
+        a = byy * inv;
+        d = bxx * inv;
+        b = -bxy * inv;
+      } else {
+        a = C(1) / fmax(bxx, C(1e-20));
+        d = C(1) / fmax(byy, C(1e-20));
+        b = C(0);
+      }
+    }
+  }
+}
+
+template <typename C>
+__device__ __forceinline__ V2<C> pre_apply(C a, C b, C d, V2<C> r) {
+  return mk2<C>(fmaT(a, r.x, b * r.y), fmaT(b, r.x, d * r.y));
+}
+
 // Elements sharing node (x, y) -- the reference's diag_count
 // (fem/preconditioner.py:19-30), here from the grid position.
 __device__ __forceinline__ int node_elem_count(int x, int y, int nx, int ny) {
