@@ -244,18 +244,6 @@ template <typename T, typename C, int PRE> struct CgCfg {
   }
 };
 
-struct UpdPlan {
-  dim3 grid;
-  int L;
-};
-UpdPlan update_plan(int nx, int ny) {
-  const int rows = (ny + 1 + UP_THREADS - 1) / UP_THREADS;
-  const int target = sm_count() * 8;
-  int strips = std::max(1, target / rows);
-  int L = std::max(4, (nx + 1 + strips - 1) / strips);
-  strips = (nx + 1 + L - 1) / L;
-  return UpdPlan{dim3(rows, strips, 1), L};
-}
 // flat update: about eight resident 256-thread CTAs per SM, grid-stride beyond
 int update_flat_ctas(int nx, int ny) {
   const int64_t total = (int64_t)(nx + 1) * (ny + 1);
@@ -271,14 +259,13 @@ dim3 blk_grid(int nx, int ny) {
 // most CTAs any PCG kernel of this grid can have (sizes the partials buffer)
 int max_ctas(const tpo_grid *g) {
   const int nx = g->nelx, ny = g->nely;
-  int m = (int)(update_plan(nx, ny).grid.x * update_plan(nx, ny).grid.y);
+  int m = update_flat_ctas(nx, ny);
   const dim3 bg = blk_grid(nx, ny);
   m = std::max(m, (int)(bg.x * bg.y));
   // the stencil plans target at most sm_count * 8 CTAs (resident <= 8 with 128 threads
   // and >= 37 KB of shared memory); bound generously without querying every variant
   const int rows = (ny + 1 + RPC - 1) / RPC;
   m = std::max(m, rows * std::max(1, (nx + 1 + 7) / 8));
-  m = std::max(m, update_flat_ctas(nx, ny));
   return m;
 }
 

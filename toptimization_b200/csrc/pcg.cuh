@@ -1,11 +1,13 @@
-// PCG kernels on the padded layout (layout.cuh). One CG iteration is two
-// launches:
-//   k_tstencil<DIR>  p = z + beta p (z from r on the fly, or the stored z of
-//                    the element-block preconditioner), Ap = K p, p.Ap;
+// PCG kernels on the padded layout (layout.cuh) for the two-launch forms
+// (the mixed form, the element-block preconditioner, and the reference's own
+// recurrence; the one-launch FP64 iteration is in cgstep.cuh):
+//   k_tstencil<DIR>  p = z + beta p (z stored by the update kernel or by the
+//                    element-block preconditioner), Ap = K p, p.Ap;
 //                    its last CTA sets alpha (or flags a breakdown).
-//   k_update / k_blockpre<UPDATE>
-//                    u += alpha p, r -= alpha Ap, z = M r, r.z, ||r||^2;
-//                    its last CTA decides convergence / refinement and beta.
+//   k_update_flat / k_blockpre<UPDATE>
+//                    u += alpha p, r -= alpha Ap, z = M r (stored), r.z,
+//                    ||r||^2; its last CTA decides convergence / refinement
+//                    and beta.
 // alpha, beta and the stop test never leave the device (PcgCtl). Every CTA
 // reads the status word first and returns at once when the solve is over, so
 // a host may enqueue more iterations than needed.
@@ -38,7 +40,6 @@ namespace tpo {
 
 constexpr int ST_THREADS = WPC * 32;  // 128 (k_blockpre)
 constexpr int TS_THREADS = ST_THREADS + 32;  // stencil: 4 consumer warps + 1 producer warp
-constexpr int UP_THREADS = 128;
 
 enum StMode { M_RAW = 0, M_DIR = 1, M_RES = 2, M_RESX = 3 };
 
@@ -364,10 +365,8 @@ __global__ void __launch_bounds__(TS_THREADS) k_tstencil(TsArgs a, int L) {
 }
 
 // ---------------------------------------------------------------------------
-// Point-preconditioner update (pointwise; a warp covers 32 rows, no halo):
-// u += alpha p, r -= alpha Ap, z = M r (z not stored), r.z and ||r||^2.
-// Columns are processed in batches of UB: a batch's loads are issued before
-// its arithmetic.
+// PCG update (pointwise): u += alpha p, r -= alpha Ap, z = M r, r.z, ||r||^2,
+// then the stop / replacement / beta logic of the step's last CTA.
 // ---------------------------------------------------------------------------
 struct UpdArgs {
   int nx, ny, P;
@@ -411,88 +410,6 @@ __device__ __forceinline__ void finish_update(PcgCtl *ctl, double rz_new, double
   ctl->rz = rz_new;
 }
 
-template <typename T, typename C, int PRE, typename X = T>
-__device__ __forceinline__ void update_run(const UpdArgs &a, int L, int bx, int by, int nb,
-                                           int bid) {
-  PcgCtl *ctl = a.ctl;
-  if (ctl->status != TPO_SOLVE_RUNNING) return;
-  const C alpha = C(ctl->alpha);
-  const T *__restrict__ p = static_cast<const T *>((ctl->it & 1) ? a.pa : a.pb);
-  const int nx = a.nx, ny = a.ny, P = a.P;
-  const int y = bx * blockDim.x + threadIdx.x;
-  const bool row_ok = y <= ny;
-  const int x0 = by * L;
-  const int x1 = min(x0 + L, nx + 1);
-  const T *__restrict__ s = static_cast<const T *>(a.s);
-  X *__restrict__ u = static_cast<X *>(a.u);
-  T *__restrict__ r = static_cast<T *>(a.r);
-  const T *__restrict__ ap = static_cast<const T *>(a.ap);
-
-  constexpr int UB = 4;
-  // element scales of column c at rows y-1, y (padded: zero outside the grid)
-  auto ld_s = [&](int c, C &sd, C &su) {
-    sd = su = C(0);
-    if (PRE != TPO_PRECOND_NONE && row_ok && c >= 0 && c < nx) {
-      const size_t e = pslot(c, y, P);
-      sd = C(s[e - 1]);
-      su = C(s[e]);
-    }
-  };
-  C ebd, ebu;
-  ld_s(x0 - 1, ebd, ebu);
-  double acc[2] = {0.0, 0.0};
-  for (int cb = x0; cb < x1; cb += UB) {
-    V2<X> uv[UB];
-    V2<T> rv[UB], pv[UB], av[UB];
-    C sd[UB], su[UB];
-    unsigned m[UB];
-#pragma unroll
-    for (int k = 0; k < UB; ++k) {
-      const int c = cb + k;
-      sd[k] = su[k] = C(0);
-      m[k] = 0;
-      if (c < x1) {
-        ld_s(c, sd[k], su[k]);
-        if (row_ok) {
-          const size_t node = pslot(c, y, P);
-          m[k] = a.mask[node];
-          uv[k] = ld2<X>(u, node);
-          rv[k] = ld2<T>(r, node);
-          pv[k] = ld2<T>(p, node);
-          av[k] = ld2<T>(ap, node);
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < UB; ++k) {
-      const int c = cb + k;
-      const C ead = ebd, eau = ebu;
-      ebd = sd[k];
-      ebu = su[k];
-      if (c < x1 && row_ok) {
-        const size_t node = pslot(c, y, P);
-        const V2<X> un = mk2<X>(X(fmaT(alpha, C(pv[k].x), C(uv[k].x))),
-                                X(fmaT(alpha, C(pv[k].y), C(uv[k].y))));
-        const V2<T> rn = mk2<T>(T(fmaT(-alpha, C(av[k].x), C(rv[k].x))),
-                                T(fmaT(-alpha, C(av[k].y), C(rv[k].y))));
-        st2<X>(u, node, un);
-        st2<T>(r, node, rn);
-        const V2<C> rc = cvt2<C, T>(rn);
-        const V2<C> z = point_precond<C, PRE>(rc, m[k], ead, eau, ebd, ebu);
-        acc[0] += (double)rc.x * z.x + (double)rc.y * z.y;
-        acc[1] += (double)rc.x * rc.x + (double)rc.y * rc.y;
-      }
-    }
-  }
-  if (!grid_reduce<2>(acc, a.part, &ctl->counter, nb, bid)) return;
-  if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
-}
-
-template <typename T, typename C, int PRE, typename X = T>
-__global__ void __launch_bounds__(UP_THREADS) k_update(UpdArgs a, int L) {
-  update_run<T, C, PRE, X>(a, L, blockIdx.x, blockIdx.y, gridDim.x * gridDim.y,
-                           blockIdx.y * gridDim.x + blockIdx.x);
-}
 
 // Same update, pointwise over the grid's nodes with a flat grid-stride loop
 // (one node per thread per pass, loads coalesced along y): no column walk and
