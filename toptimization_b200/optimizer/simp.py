@@ -144,6 +144,46 @@ class SimpDesign:
         return self.rho.cpu().numpy()
 
 
+class GraphDesign:
+    """One design run through the batched engine (`toptimization_b200.batch`)
+    as a batch of one: each OC iteration is a single CUDA graph launch in which
+    a conditional while node runs the PCG loop on the device (no host round
+    trip inside the iteration). Mixed precision, density filter and a point
+    preconditioner only. Same `step()` / `density()` interface as
+    `SimpDesign`."""
+
+    def __init__(self, problem, device=None, preconditioner: str | None = None):
+        from ..batch import Batch
+        pr = problem
+        pre = preconditioner or pr.preconditioner
+        if pr.filter_type != "density":
+            raise ValueError("engine='graph' runs the density filter only")
+        if pre not in ("jacobi", "nodal_block_jacobi", "none"):
+            raise ValueError("engine='graph' takes a point preconditioner")
+        self.problem = pr
+        self.precision = "mixed"
+        self.preconditioner = pre
+        self.batch = Batch(1, preconditioner=pre, use_graph=True, device=device)
+        self.slot = self.batch.add(pr)
+        self.it = 0
+
+    def step(self) -> IterationRecord:
+        t0 = time.perf_counter()
+        self.batch.step()
+        h = self.batch.history(self.slot)
+        self.it = len(h["compliance"])
+        i = self.it - 1
+        status = _lib.SOLVE_STATUS.get(int(h["pcg_status"][i]), str(int(h["pcg_status"][i])))
+        info = SolveInfo(status, int(h["cg_iters"][i]), int(h["outer_iters"][i]),
+                         int(h["cg_iters"][i]), float("nan"))
+        return IterationRecord(self.it, float(h["compliance"][i]), float(h["volume"][i]),
+                               float(h["change"][i]), int(h["cg_iters"][i]), info,
+                               time.perf_counter() - t0)
+
+    def density(self) -> np.ndarray:
+        return self.batch.density(self.slot).reshape(-1)
+
+
 def _check_backend(backend: str) -> None:
     if backend not in ("auto", "cuda"):
         raise ValueError(f"Unknown backend '{backend}': toptimization_b200 runs on CUDA only")
@@ -154,7 +194,8 @@ def _check_backend(backend: str) -> None:
 def run(problem, backend: str = "auto", live_viz: bool = True,
         viz_callback: Callable | None = None, *, precision: str | None = None,
         preconditioner: str | None = None, device=None, verbose: bool = True,
-        save: bool = True, history: RunHistory | None = None) -> np.ndarray:
+        save: bool = True, history: RunHistory | None = None,
+        engine: str = "direct") -> np.ndarray:
     """Run SIMP topology optimisation; returns the final design density as an
     array of shape (nelx, nely), FP64 (reference simp.py:19-41,309-312).
 
@@ -162,12 +203,22 @@ def run(problem, backend: str = "auto", live_viz: bool = True,
     (simp.py:213-214). `live_viz` is accepted for compatibility; there is no
     window (headless). `precision` overrides `problem.precision`
     ("fp64" | "mixed"); `history` (optional) receives every per-iteration record.
+    `engine="graph"` runs each OC iteration as one CUDA graph (mixed precision,
+    density filter, point preconditioner; see `GraphDesign`).
     """
     _check_backend(backend)
     pr = problem
     if pr.dim != 2:
         raise NotImplementedError("toptimization_b200 implements the 2D Q4 path only")
-    design = SimpDesign(pr, device=device, precision=precision, preconditioner=preconditioner)
+    if engine == "graph":
+        if (precision or pr.precision) != "mixed":
+            raise ValueError("engine='graph' runs the mixed-precision form")
+        design = GraphDesign(pr, device=device, preconditioner=preconditioner)
+    elif engine == "direct":
+        design = SimpDesign(pr, device=device, precision=precision,
+                            preconditioner=preconditioner)
+    else:
+        raise ValueError(f"unknown engine {engine!r}")
     hist = history if history is not None else RunHistory()
     if verbose:
         print(f"[toptimization_b200] {pr.name}: {pr.nelx}x{pr.nely}, n_dofs={pr.n_dofs:,}, "
