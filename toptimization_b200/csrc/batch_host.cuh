@@ -665,18 +665,23 @@ int tpo_batch_time_steps(tpo_batch *b, int32_t steps, tpo_stream s, float *ms_ou
   if (b->nctas[BK_FILTER] == 0) return fail(TPO_ERR_ARGS, "no active design");
   if ((rc = batch_prefix(b, st))) return rc;
   if ((rc = batch_body_any(b, st, 0, 0))) return rc;  // FP64 residual, first steps
-  cudaEvent_t e0, e1;
-  TPO_CK(cudaEventCreate(&e0));
-  TPO_CK(cudaEventCreate(&e1));
-  TPO_CK(cudaEventRecord(e0, st));
+  // the events are released on every path out of the timed region
+  struct Events {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  TPO_CK(cudaEventCreate(&ev.e[0]));
+  TPO_CK(cudaEventCreate(&ev.e[1]));
+  TPO_CK(cudaEventRecord(ev.e[0], st));
   for (int i = 0; i < steps; i += kBatchSteps)
     if ((rc = batch_body_any(b, st, 0, 0))) return rc;
-  TPO_CK(cudaEventRecord(e1, st));
-  TPO_CK(cudaEventSynchronize(e1));
+  TPO_CK(cudaEventRecord(ev.e[1], st));
+  TPO_CK(cudaEventSynchronize(ev.e[1]));
   float ms = 0.f;
-  TPO_CK(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  TPO_CK(cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]));
   *ms_out = ms;
   return TPO_OK;
 }
