@@ -113,8 +113,12 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
   const bool own_row = lane >= 1 && lane <= RPW && y <= ny;
   const int x0 = by * L;
   const int x1 = min(x0 + L, nx + 1);
-  const int cA = x0 - 2;               // first staged column
-  const int NC = x1 - cA + 1;          // staged columns cA..x1
+  // Only a direction kernel that rebuilds a point preconditioner at node
+  // x0-1 needs element column x0-2: it stages that column's scales alone.
+  // Every other mode starts at x0-1 with nodes and scales.
+  constexpr bool SCALE_COL = MODE == M_DIR && PRE != TPO_PRECOND_BLOCK_JACOBI;
+  const int cA = x0 - (SCALE_COL ? 2 : 1);  // first staged column
+  const int NC = x1 - cA + 1;               // staged columns cA..x1
   const int NGRP = (NC + G - 1) / G;
   const int ms = (Y0 + LEAD - 1) & ~15;  // first staged mask byte of a column
 
@@ -136,14 +140,15 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     for (int k = 0; k < G; ++k) {
       const int c = cA + g * G + k;
       if (c > x1) break;
-      if (c > cA && c >= 0 && c <= nx) bytes += Geo::CNB * (Geo::HAS_B ? 2 : 1) + Geo::CMB;
+      if ((!SCALE_COL || c > cA) && c >= 0 && c <= nx)
+        bytes += Geo::CNB * (Geo::HAS_B ? 2 : 1) + Geo::CMB;
       if (c >= 0 && c < nx) bytes += Geo::CEB;
     }
     mbar_arrive_expect_tx(&full[g % NG], bytes);
     for (int k = 0; k < G; ++k) {
       const int c = cA + g * G + k;
       if (c > x1) break;
-      if (c > cA && c >= 0 && c <= nx) {
+      if ((!SCALE_COL || c > cA) && c >= 0 && c <= nx) {
         const size_t col = (size_t)c * P + Y0 + N_OFF;
         bulk_g2s(sb + k * Geo::CNB, ga + 2 * col, Geo::CNB, &full[g % NG]);
         if constexpr (Geo::HAS_B)
@@ -213,7 +218,7 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     const T *colS = reinterpret_cast<const T *>(sb + G * Geo::CNB * (Geo::HAS_B ? 2 : 1) +
                                                 kk * Geo::CEB);
     const uint8_t *colM = sb + G * Geo::CNB * (Geo::HAS_B ? 2 : 1) + G * Geo::CEB + kk * Geo::CMB;
-    const bool node_ok = c > cA && c >= 0 && c <= nx;  // column cA stages scales only
+    const bool node_ok = (!SCALE_COL || c > cA) && c >= 0 && c <= nx;
     const bool elem_ok = c >= 0 && c < nx;
     const C scd = elem_ok ? C(colS[e_idx]) : C(0);      // element (c, y-1)
     const C scu = elem_ok ? C(colS[e_idx + 1]) : C(0);  // element (c, y)
