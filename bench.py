@@ -67,9 +67,11 @@ def parse_args():
     ap.add_argument("--recurrence", choices=["auto", "standard", "single"], default="auto",
                     help="PCG iteration form: one launch per iteration (auto) or the "
                          "reference's two-step recurrence (standard)")
-    ap.add_argument("--workload", choices=["bridge", "batch", "serve"], default="bridge",
+    ap.add_argument("--workload", choices=["bridge", "batch", "serve", "solid3d"],
+                    default="bridge",
                     help="bridge: the 2048x1024 headline line; batch: uneven designs "
-                         "advanced together; serve: a Poisson request stream")
+                         "advanced together; serve: a Poisson request stream; solid3d: "
+                         "the 3D H8 cantilever (examples/cantilever3d_128x64x64.yaml)")
     ap.add_argument("--designs", type=int, default=64, help="batch: number of designs")
     ap.add_argument("--oc-iters", type=int, default=50, help="batch/serve: OC iterations")
     ap.add_argument("--seed", type=int, default=0)
@@ -611,12 +613,150 @@ def run_serve(args):
     return 0
 
 
+SOLID3D_YAML = REPO / "examples" / "cantilever3d_128x64x64.yaml"
+SOLID3D_UNIT = "OC iter/s"
+SOLID3D_CPU_CG = 12
+# FP64 FMA issue of the B200: 148 SMs x 64 FP64 FMA/clk x 2 flops x 1.965 GHz
+FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+
+
+def cpu_sample_3d(pr, cg_per_oc):
+    """The oracle (NumPy, matrix-free element operator, Jacobi PCG) on the full
+    3D grid: one OC iteration with the PCG capped at SOLID3D_CPU_CG
+    iterations, PCG time scaled to `cg_per_oc` iterations."""
+    import numpy as np
+    from oracle import simp64 as O
+    from toptimization_b200.material import compute_Ke_3d
+    from toptimization_b200.mesh import force_vector
+    try:
+        from threadpoolctl import threadpool_info
+        cores = max([i.get("num_threads", 1) for i in threadpool_info()] or [1])
+    except Exception:
+        cores = 1
+    mesh = O.Mesh3D(pr.nelx, pr.nely, pr.nelz, compute_Ke_3d(pr.E, pr.nu), pr.fixed_dofs)
+    f = force_vector(pr)
+    t0 = time.perf_counter()
+    H, Hs = O.filter_matrix(pr.nelx, pr.nely, pr.rmin, pr.nelz)
+    t_setup = time.perf_counter() - t0
+    rho = np.full(mesh.n_elem, float(pr.volfrac))
+    t0 = time.perf_counter()
+    phys = O.density_filter(H, Hs, rho)
+    scale = O.simp_scale(phys, pr.E_min, pr.penalty)
+    t1 = time.perf_counter()
+    res = O.pcg(mesh, scale, f, np.zeros(mesh.n_dofs), pr.cg_tol, SOLID3D_CPU_CG, "jacobi",
+                assemble=False)
+    t2 = time.perf_counter()
+    dc, _ = O.sensitivity(mesh, res.u, phys, pr.E_min, pr.penalty)
+    dcf = O.density_filter(H, Hs, dc)
+    O.oc_update(rho, dcf, pr.volfrac, pr.move_limit)
+    t3 = time.perf_counter()
+    per_cg = (t2 - t1) / max(res.iters, 1)
+    t = (t1 - t0) + (t3 - t2) + per_cg * cg_per_oc
+    return {"value": round(1.0 / t, 6), "unit": SOLID3D_UNIT, "cores": int(cores),
+            "kind": "port",
+            "sample": (f"NumPy oracle (oracle/simp64.py: matrix-free element operator, Jacobi "
+                       f"PCG, FP64) on the full {pr.nelx}x{pr.nely}x{pr.nelz} grid: one OC "
+                       f"iteration with the PCG capped at {SOLID3D_CPU_CG} iterations, PCG "
+                       f"time scaled to {cg_per_oc} iterations per OC iteration; filter "
+                       f"matrix setup ({t_setup:.1f} s) not counted"),
+            "seconds_per_oc_iter": round(t, 3)}
+
+
+def run_solid3d(args):
+    """OC iterations/s of the 3D (H8) loop: FP64 Jacobi PCG, density filter."""
+    import numpy as np
+    import torch
+    from toptimization_b200 import _lib
+    from toptimization_b200.csrc import build as csrc_build
+    from toptimization_b200.optimizer.simp import SimpDesign, run
+    from toptimization_b200.problem import load_problem
+    csrc_build.build()
+    lib = _lib.load()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    pr = load_problem(SOLID3D_YAML)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    d = SimpDesign(pr, device=dev, precision="fp64", preconditioner="jacobi")
+    for _ in range(args.warmup):
+        d.step()
+    lib.tpo_profile_reset()
+    with ClockSampler(0) as clocks:
+        times, recs = time_steps(d, args.steps, 0, flush, torch)
+    launches = _lib.profile_read()["launches"]
+    kern = profile_pass(d, lib, _lib, torch)
+    del d
+    t = sum(times)
+    value = args.steps / (t / 1e3)
+    cg_mean = float(np.mean([r.cg_iters for r in recs]))
+    peak, peak_kind = measured_peak()
+    nn = pr.n_nodes
+    names = {"dir": "k_hex_gather<DIR> (p = z + beta p, K p over the 27-node neighbourhood, "
+                    "p.Kp)",
+             "update": "k_hex_update<jacobi> (u, r update, z = r / diag, r.z, ||r||^2)"}
+    key = max(kern, key=lambda k: kern[k]["total_ms"])
+    kd = kern[key]
+    flops = 2 * 600 * nn if key == "dir" else 8 * pr.n_dofs
+    tflops = flops / (kd["avg_us"] * 1e-6) / 1e12
+    roofline = {"bound": "hbm", "kernel": names[key], "achieved": kd["gbs"], "peak": peak,
+                "unit": "GB/s", "frac": round(kd["gbs"] / peak, 3) if kd["gbs"] else None,
+                "traffic": ncu_traffic("solid3d_" + key),
+                "bytes_per_launch": kd["bytes_per_launch"], "avg_launch_us": kd["avg_us"],
+                "launches_timed": kd["launches"], "peak_kind": peak_kind,
+                "fp64": {"achieved_tflops": round(tflops, 2),
+                         "nominal_tflops": round(FP64_NOMINAL_TFLOPS, 1),
+                         "frac": round(tflops / FP64_NOMINAL_TFLOPS, 3),
+                         "flops_per_launch": flops,
+                         "note": "the gather kernel issues 600 FP64 FMAs per node; the FP64 "
+                                 "pipe, not HBM, bounds it"},
+                "kernels": kern}
+    e2e = None
+    if not args.no_e2e:
+        pr_e = load_problem(SOLID3D_YAML)
+        pr_e.max_iter = args.warmup + args.steps
+        pr_e.tol = 0.0
+        got = []
+        t0 = time.perf_counter()
+        run(pr_e, backend="cuda", live_viz=False, verbose=False, save=False,
+            viz_callback=lambda rho, it, c, v: got.append(rho.nbytes))
+        torch.cuda.synchronize()
+        t_e = time.perf_counter() - t0
+        h2d = 8 * pr.n_dofs + pr.n_nodes + 2 * 576 * 8
+        e2e = {"value": round(pr_e.max_iter / t_e, 4), "unit": SOLID3D_UNIT,
+               "h2d_bytes_per_step": int(h2d / pr_e.max_iter),
+               "d2h_bytes_per_step": int(np.mean(got)) + 5 * 8,
+               "note": (f"simp.run() from a host Problem to the host density, {pr_e.max_iter} "
+                        "OC iterations from the initial design")}
+    line = {"metric": f"OC iter/s @3D cantilever {pr.nelx}x{pr.nely}x{pr.nelz} H8 FP64",
+            "value": round(value, 4), "unit": SOLID3D_UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(t / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": f"synthetic (the 3D cantilever of {SOLID3D_YAML.relative_to(REPO)})",
+            "config": {"workload": f"3D cantilever {pr.nelx}x{pr.nely}x{pr.nelz} H8 "
+                                   f"({SOLID3D_YAML.relative_to(REPO)})",
+                       "n_elem": pr.n_elem, "n_dofs": pr.n_dofs, "preconditioner": "jacobi",
+                       "cg_tol": pr.cg_tol, "rmin": pr.rmin, "volfrac": pr.volfrac,
+                       "oc_iterations_timed": f"{args.warmup + 1}..{args.warmup + args.steps}",
+                       "step": "one OC iteration (filter, PCG, sensitivity, dc filter, OC)",
+                       "l2": "flushed between timed steps (256 MiB write)"},
+            "cg_iters": [r.cg_iters for r in recs], "compliance": [r.compliance for r in recs],
+            "gpu_launches": int(launches), "roofline": roofline, "clocks": clocks.summary()}
+    if e2e is not None:
+        line["e2e"] = e2e
+    if not args.no_cpu:
+        line["cpu_baseline"] = cpu_sample_3d(pr, int(round(cg_mean)))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global _RECURRENCE
     args = parse_args()
     _RECURRENCE = args.recurrence
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "solid3d":
+        return run_solid3d(args)
     if args.workload == "serve":
         return run_serve(args)
     if args.case == "pcg":

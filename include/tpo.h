@@ -313,6 +313,68 @@ int tpo_batch_states(tpo_batch *b, int32_t n, int32_t *it_out, int32_t *active_o
  * advances the designs' PCG state, so use a scratch batch). */
 int tpo_batch_time_steps(tpo_batch *b, int32_t steps, tpo_stream s, float *ms_out);
 
+/* ---- 3D: trilinear hexahedra (H8) ------------------------------------------
+ * Structured nelx x nely x nelz grid of unit cubes in the reference's
+ * numbering (src/toptimization/mesh.py:68-112), used as it is (no padding):
+ *   node (ix, iy, iz)    -> (ix*(nely+1) + iy)*(nelz+1) + iz   (iz fastest)
+ *   nodal vector v       -> v[3*node + {0:x, 1:y, 2:z}]       (3*(nelx+1)(nely+1)(nelz+1))
+ *   element (ex, ey, ez) -> (ex*nely + ey)*nelz + ez
+ *   fixed mask           -> uint8 per node, bit0/1/2 = x/y/z fixed
+ * FP64 throughout; nodal vectors need 8-byte alignment. The reference runs
+ * these through the same entry points as 2D with dim == 3 (fem/kernels.py
+ * compute_*_3d, fem/fused_kernels.py:59-94, fem/preconditioner.py:112-156,
+ * optimizer/filter.py:75-97); here they are separate functions. */
+typedef struct tpo_grid3 {
+  int32_t nelx, nely, nelz, pad;
+  double e_min;    /* scale = e_min + rho^penalty (1 - e_min) */
+  double penalty;
+} tpo_grid3;
+
+/* 24x24 H8 stiffness (row-major, DOFs [x,y,z] per corner in mesh.py:87-96
+ * order), its regularised inverse (Ke + alpha I)^-1 and alpha (reference
+ * material.py:89-171, fem/fields.py:133-143), into constant memory of the
+ * CURRENT device. Must be called once per device before any tpo3_* kernel. */
+int tpo_set_stiffness3(const double ke[576], const double ke_inv[576], double alpha_reg);
+
+/* ap = K(rho) p, identity rows at fixed DOFs; *pap_out (device, nullable) =
+ * p.ap. Replaces compute_matvec_3d / matvec_and_dot_3d (fem/kernels.py:179-212,
+ * fem/fused_kernels.py:59-94). */
+size_t tpo3_matvec_workspace_bytes(const tpo_grid3 *g);
+int tpo3_matvec_f64(const tpo_grid3 *g, const double *rho, const uint8_t *fixed,
+                    const double *p, double *ap, double *pap_out,
+                    void *ws, size_t ws_bytes, tpo_stream s);
+
+/* PCG solve K(rho) u = f with the reference's rules (fem/solver.py:27-159):
+ * precond TPO_PRECOND_NONE / JACOBI / BLOCK_JACOBI, precision FP64,
+ * recurrence AUTO or STANDARD (two launches per iteration; three with the
+ * element-block preconditioner). BLOCKING, like tpo_pcg_solve. */
+size_t tpo3_pcg_workspace_bytes(const tpo_grid3 *g, const tpo_solve_cfg *c);
+int tpo3_pcg_solve(const tpo_grid3 *g, const tpo_solve_cfg *c,
+                   const double *rho_phys, const double *f, const uint8_t *fixed,
+                   double *u, void *ws, size_t ws_bytes,
+                   tpo_solve_result *out, tpo_stream s);
+
+/* dc and compliance as tpo_sensitivity (fem/kernels.py:275-308). */
+size_t tpo3_sensitivity_workspace_bytes(const tpo_grid3 *g);
+int tpo3_sensitivity(const tpo_grid3 *g, const double *rho_phys, const double *u,
+                     double *dc, double *compliance_out,
+                     void *ws, size_t ws_bytes, tpo_stream s);
+
+/* Hat-weight filters over the box |dx|,|dy|,|dz| <= ceil(rmin) <= 8
+ * (optimizer/filter.py:75-97,106-171); same formulas as the 2D ones. */
+int tpo3_density_filter(const tpo_grid3 *g, double rmin, const double *x, double *out,
+                        tpo_stream s);
+int tpo3_sensitivity_filter(const tpo_grid3 *g, double rmin, const double *rho,
+                            const double *dc, double *out, tpo_stream s);
+
+/* OC update over the nelx*nely*nelz elements, as tpo_oc_update
+ * (optimizer/oc.py:21-93). */
+size_t tpo3_oc_workspace_bytes(const tpo_grid3 *g);
+int tpo3_oc_update(const tpo_grid3 *g, double volfrac, double move,
+                   const double *rho_in, const double *dc, const double *dv,
+                   double *rho_out, double *result_out,
+                   void *ws, size_t ws_bytes, tpo_stream s);
+
 #ifdef __cplusplus
 }
 #endif

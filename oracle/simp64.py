@@ -22,27 +22,55 @@ from dataclasses import dataclass, field
 import numpy as np
 import scipy.sparse as sp
 
-from toptimization_b200.material import compute_Ke_2d, regularized_inverse
-from toptimization_b200.mesh import build_edof_2d
+from toptimization_b200.material import compute_Ke, compute_Ke_2d, regularized_inverse
+from toptimization_b200.mesh import build_edof_2d, build_edof_3d
 
 
 @dataclass
 class Mesh2D:
+    """Structured Q4 mesh (`mesh.py:33-65`); with `nelz` set, the H8 mesh
+    (`mesh.py:68-112`, node (ix,iy,iz) -> (ix(nely+1)+iy)(nelz+1)+iz, 24 DOFs
+    per element). Every function below works on either through `edof`."""
     nelx: int
     nely: int
     Ke: np.ndarray
     fixed_dofs: np.ndarray
+    nelz: int = 0
     edof: np.ndarray = field(init=False)
 
     def __post_init__(self):
-        self.edof = build_edof_2d(self).astype(np.int64)
-        self.n_elem = self.nelx * self.nely
-        self.n_nodes = (self.nelx + 1) * (self.nely + 1)
-        self.n_dofs = 2 * self.n_nodes
+        self.dim = 3 if self.nelz else 2
+        if self.dim == 2:
+            self.edof = build_edof_2d(self).astype(np.int64)
+            self.n_elem = self.nelx * self.nely
+            self.n_nodes = (self.nelx + 1) * (self.nely + 1)
+        else:
+            self.edof = build_edof_3d(self).astype(np.int64)
+            self.n_elem = self.nelx * self.nely * self.nelz
+            self.n_nodes = (self.nelx + 1) * (self.nely + 1) * (self.nelz + 1)
+        self.n_dofs = self.dim * self.n_nodes
         self.is_fixed = np.zeros(self.n_dofs, dtype=bool)
         self.is_fixed[np.asarray(self.fixed_dofs, dtype=np.int64)] = True
-        self._rows = np.repeat(self.edof, 8, axis=1).reshape(-1)
-        self._cols = np.tile(self.edof, (1, 8)).reshape(-1)
+
+    # COO index arrays of the assembled matrices, built on first use (E*dpe^2
+    # entries: too large to keep for big 3D grids, which use matvec_free)
+    @property
+    def _rows(self):
+        if not hasattr(self, "_rows_c"):
+            dpe = self.edof.shape[1]
+            self._rows_c = np.repeat(self.edof, dpe, axis=1).reshape(-1)
+        return self._rows_c
+
+    @property
+    def _cols(self):
+        if not hasattr(self, "_cols_c"):
+            self._cols_c = np.tile(self.edof, (1, self.edof.shape[1])).reshape(-1)
+        return self._cols_c
+
+
+def Mesh3D(nelx, nely, nelz, Ke, fixed_dofs) -> Mesh2D:
+    """The H8 mesh (see Mesh2D)."""
+    return Mesh2D(nelx, nely, Ke, fixed_dofs, nelz=nelz)
 
 
 def simp_scale(rho, E_min, penalty):
@@ -67,6 +95,26 @@ def assemble_K(mesh: Mesh2D, scale: np.ndarray) -> sp.csr_matrix:
 def matvec(mesh, rho, p, E_min, penalty):
     """K(rho) p  (`fem/kernels.py:143-176`)."""
     return assemble_K(mesh, simp_scale(rho, E_min, penalty)) @ p
+
+
+def matvec_free(mesh, scale, p):
+    """K(rho) p element by element, without assembling K: the reference's
+    matrix-free form (`fem/kernels.py:143-212`: gather p_e, Ke p_e, scale,
+    scatter-add; fixed rows Ap = p), with the scatter as one bincount."""
+    ke = (p[mesh.edof] @ mesh.Ke.T) * scale[:, None]
+    ap = np.bincount(mesh.edof.reshape(-1), weights=ke.reshape(-1), minlength=mesh.n_dofs)
+    ap[mesh.is_fixed] = p[mesh.is_fixed]
+    return ap
+
+
+class FreeOperator:
+    """`K @ p` through matvec_free (for grids too large to assemble)."""
+
+    def __init__(self, mesh, scale):
+        self.mesh, self.scale = mesh, scale
+
+    def __matmul__(self, p):
+        return matvec_free(self.mesh, self.scale, p)
 
 
 def jacobi_diag(mesh, scale):
@@ -148,7 +196,8 @@ class SolveResult:
     rr: float
 
 
-def pcg(mesh, scale, f, u0, tol, max_iter, precond="jacobi") -> SolveResult:
+def pcg(mesh, scale, f, u0, tol, max_iter, precond="jacobi",
+        assemble: bool = True) -> SolveResult:
     """PCG exactly as the reference drives it (`fem/solver.py:27-159`):
     warm start with fixed DOFs zeroed, true initial residual, breakdown when
     |p.Ap| < 1e-30, recursive-residual stop ||r||^2 < (tol ||f||)^2 tested
@@ -159,7 +208,7 @@ def pcg(mesh, scale, f, u0, tol, max_iter, precond="jacobi") -> SolveResult:
     if f_norm < 1e-30:
         return SolveResult(np.zeros_like(f), 0, "zero_rhs", 0.0)
     tol_sq = (tol * f_norm) ** 2
-    K = assemble_K(mesh, scale)
+    K = assemble_K(mesh, scale) if assemble else FreeOperator(mesh, scale)
     M = Preconditioner(precond, mesh, scale)
     u = u0.copy()
     u[mesh.is_fixed] = 0.0
@@ -196,11 +245,14 @@ def sensitivity(mesh, u, rho, E_min, penalty):
     return dc, float(np.sum(simp_scale(rho, E_min, penalty) * uKu))
 
 
-def filter_matrix(nelx, nely, rmin) -> tuple[sp.csr_matrix, np.ndarray]:
+def filter_matrix(nelx, nely, rmin, nelz=0) -> tuple[sp.csr_matrix, np.ndarray]:
     """Hat-weight neighbour matrix H and row sums Hs
     (`optimizer/filter.py:22-103`): w = max(0, rmin - |c_e - c_j|) over the box
     |dx|,|dy| <= ceil(rmin) clipped to the domain, kept where w > 0; columns in
-    the reference's (jx outer, jy inner) order."""
+    the reference's (jx outer, jy inner) order. With nelz, the 3D box
+    (`filter.py:75-97`, element (ex,ey,ez) -> (ex nely + ey) nelz + ez)."""
+    if nelz:
+        return _filter_matrix_3d(nelx, nely, nelz, rmin)
     R = math.ceil(rmin)
     ex, ey = np.divmod(np.arange(nelx * nely), nely)
     rows, cols, vals = [], [], []
@@ -218,6 +270,30 @@ def filter_matrix(nelx, nely, rmin) -> tuple[sp.csr_matrix, np.ndarray]:
                       shape=(nelx * nely, nelx * nely))
     H.sort_indices()
     return H, H @ np.ones(nelx * nely)
+
+
+def _filter_matrix_3d(nelx, nely, nelz, rmin):
+    R = math.ceil(rmin)
+    n = nelx * nely * nelz
+    e = np.arange(n)
+    ex, ey, ez = e // (nely * nelz), (e // nelz) % nely, e % nelz
+    rows, cols, vals = [], [], []
+    for dx in range(-R, R + 1):
+        for dy in range(-R, R + 1):
+            for dz in range(-R, R + 1):
+                w = rmin - math.sqrt(float(dx * dx + dy * dy + dz * dz))
+                if not w > 0.0:
+                    continue
+                jx, jy, jz = ex + dx, ey + dy, ez + dz
+                ok = ((jx >= 0) & (jx < nelx) & (jy >= 0) & (jy < nely)
+                      & (jz >= 0) & (jz < nelz))
+                rows.append(np.flatnonzero(ok))
+                cols.append(((jx * nely + jy) * nelz + jz)[ok])
+                vals.append(np.full(ok.sum(), w))
+    H = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(n, n))
+    H.sort_indices()
+    return H, H @ np.ones(n)
 
 
 def density_filter(H, Hs, x):
@@ -265,17 +341,18 @@ class RunResult:
 
 
 def run(problem, max_iter=None, callback=None) -> RunResult:
-    """The SIMP loop of `optimizer/simp.py:108-109,141-219`: density filter ->
+    """The SIMP loop of `optimizer/simp.py:108-109,141-219` (2D or 3D): density filter ->
     PCG on the physical density (warm start from it > 1) -> sensitivity ->
     dc projection -> OC on the design density -> volume; early stop when
     it > 5 and change < tol. The sensitivity-filter branch (:174-189) too."""
     pr = problem
-    Ke = compute_Ke_2d(pr.E, pr.nu)
-    mesh = Mesh2D(pr.nelx, pr.nely, Ke, pr.fixed_dofs)
+    Ke = compute_Ke(pr.E, pr.nu, pr.dim)
+    nelz = pr.nelz if pr.dim == 3 else 0
+    mesh = Mesh2D(pr.nelx, pr.nely, Ke, pr.fixed_dofs, nelz=nelz)
     f = np.zeros(mesh.n_dofs)
     np.add.at(f, np.asarray(pr.force_dofs, dtype=np.int64), np.asarray(pr.force_values, float))
     f[mesh.is_fixed] = 0.0
-    H, Hs = filter_matrix(pr.nelx, pr.nely, pr.rmin)
+    H, Hs = filter_matrix(pr.nelx, pr.nely, pr.rmin, nelz)
     rho = np.full(mesh.n_elem, float(pr.volfrac))
     u_prev = np.zeros(mesh.n_dofs)
     out = RunResult(rho, [], [], [], [], [])

@@ -12,8 +12,11 @@ What is recorded, all from the reference's own code:
                       element-block preconditioner, sensitivity, the three
                       filters, the OC update, a PCG solve per preconditioner)
                       on a seeded 12x5 cantilever.
+  ref_kernels3d.npz   the same single calls through the reference's 3D (H8)
+                      kernels on a seeded 5x3x2 cantilever.
   ref_run_*.npz       whole `simp.run` optimisations: compliance, volume,
-                      change and CG-count histories plus final densities.
+                      change and CG-count histories plus final densities
+                      (ref_run_3d_*: the 3D loop on an 8x4x3 cantilever).
 
 The kernels run under `taichi_fp64_shim` (Taichi is not installable here), with
 every value in FP64; see that module's header for exactly what it implements.
@@ -109,7 +112,33 @@ def _small_problem(nelx=12, nely=5, rmin=1.5, pre="jacobi"):
                    output_format="png"), nn
 
 
+def _small_problem_3d(nelx=5, nely=3, nelz=2):
+    """Left face clamped; y load on the right face's bottom edge."""
+    from toptimization.problem import Problem
+    ny1, nz1 = nely + 1, nelz + 1
+    fixed = np.arange(0, 3 * ny1 * nz1)
+    load = np.array([3 * ((nelx * ny1 + 0) * nz1 + iz) + 1 for iz in range(nz1)])
+    return Problem(name="k3", dim=3, nelx=nelx, nely=nely, nelz=nelz, E=1.0, nu=0.3,
+                   E_min=1e-9, fixed_dofs=fixed, force_dofs=load,
+                   force_values=np.full(load.size, -1.0 / load.size), volfrac=0.4,
+                   penalty=3.0, rmin=1.5, filter_type="density", max_iter=1, tol=0.0,
+                   move_limit=0.2, max_cg_iter=500, cg_tol=1e-10, preconditioner="jacobi",
+                   output_dir=Path(tempfile.mkdtemp()), save_interval=10 ** 6,
+                   output_format="png")
+
+
 def _kernels(ref_src: str) -> dict:
+    _import_reference(ref_src)
+    pr, _ = _small_problem()
+    return _kernel_suite(ref_src, pr, 2, 20261203, (1.5, 2.5, 4.0))
+
+
+def _kernels3d(ref_src: str) -> dict:
+    _import_reference(ref_src)
+    return _kernel_suite(ref_src, _small_problem_3d(), 3, 20261204, (1.5, 2.2))
+
+
+def _kernel_suite(ref_src: str, pr, dim: int, seed: int, rmin_list) -> dict:
     _import_reference(ref_src)
     import math
     from toptimization.fem import fields as F, kernels as K, fused_kernels as FK
@@ -118,19 +147,20 @@ def _kernels(ref_src: str) -> dict:
     from toptimization.mesh import build_edof, element_centers
     from toptimization.material import compute_Ke
 
-    rng = np.random.default_rng(20261203)
-    pr, nn = _small_problem()
+    rng = np.random.default_rng(seed)
     E, N = pr.n_elem, pr.n_dofs
-    Ke = compute_Ke(1.0, 0.3, 2)
+    Ke = compute_Ke(1.0, 0.3, dim)
     edof = build_edof(pr)
-    rmin_list = (1.5, 2.5, 4.0)
+    dpe = Ke.shape[0]
 
     def alloc(rmin):
-        F.allocate(n_dofs=N, n_elem=E, dpe=8, max_neighbors=(2 * math.ceil(rmin) + 1) ** 2,
+        F.allocate(n_dofs=N, n_elem=E, dpe=dpe,
+                   max_neighbors=(2 * math.ceil(rmin) + 1) ** dim,
                    Ke_np=Ke, edof_np=edof, fixed_dofs=pr.fixed_dofs,
                    force_dofs=pr.force_dofs, force_values=pr.force_values)
 
     out = {"nelx": np.int64(pr.nelx), "nely": np.int64(pr.nely),
+           "nelz": np.int64(pr.nelz),
            "fixed": pr.fixed_dofs, "force_dofs": pr.force_dofs,
            "force_values": pr.force_values}
     rho = rng.uniform(0.001, 1.0, E)
@@ -142,22 +172,22 @@ def _kernels(ref_src: str) -> dict:
     alloc(1.5)
     F.rho.from_numpy(rho)
     F.p.from_numpy(p)
-    K.compute_matvec(F.p, F.Ap, F.rho, F.Ke, F.edof, F.is_fixed, Emin, pen, E, 2)
+    K.compute_matvec(F.p, F.Ap, F.rho, F.Ke, F.edof, F.is_fixed, Emin, pen, E, dim)
     out["Ap"] = F.Ap.to_numpy()
     out["pAp"] = np.float64(FK.matvec_and_dot(F.p, F.Ap, F.rho, F.Ke, F.edof, F.is_fixed,
-                                              Emin, pen, E, 2))
-    K.compute_diagonal(F.diag, F.rho, F.Ke, F.edof, F.is_fixed, Emin, pen, E, 2)
+                                              Emin, pen, E, dim))
+    K.compute_diagonal(F.diag, F.rho, F.Ke, F.edof, F.is_fixed, Emin, pen, E, dim)
     out["diag"] = F.diag.to_numpy()
-    PC.setup(F.edof, F.diag_count, E, 2)
+    PC.setup(F.edof, F.diag_count, E, dim)
     out["diag_count"] = F.diag_count.to_numpy()
     F.r.from_numpy(p2)
     rz = PC.apply_and_rz(F.r, F.z, F.rho, F.Ke_inv, F.edof, F.diag_count, F.is_fixed,
-                         F._dot_result, Emin, pen, F.KE_ALPHA_REG, E, 2)
+                         F._dot_result, Emin, pen, F.KE_ALPHA_REG, E, dim)
     out["bj_z"] = F.z.to_numpy()
     out["bj_rz"] = np.float64(rz)
     out["bj_rr"] = np.float64(F._dot_result[None])
     F.u.from_numpy(p)
-    c = K.compute_sensitivity(F.u, F.rho, F.dc, F.dv, F.Ke, F.edof, Emin, pen, E, 2)
+    c = K.compute_sensitivity(F.u, F.rho, F.dc, F.dv, F.Ke, F.edof, Emin, pen, E, dim)
     out["sens_dc"] = F.dc.to_numpy()
     out["sens_c"] = np.float64(c)
     out["volume"] = np.float64(K.compute_volume(F.rho, E))
@@ -195,15 +225,15 @@ def _kernels(ref_src: str) -> dict:
         alloc(1.5)
         F.rho.from_numpy(rho)
         if pre == "block_jacobi":
-            PC.setup(F.edof, F.diag_count, E, 2)
+            PC.setup(F.edof, F.diag_count, E, dim)
         K.fill_scalar(F.u_prev, 0.0)
-        n = solver.solve(E_min=Emin, penalty=pen, dim=2, max_iter=500, tol=1e-10,
+        n = solver.solve(E_min=Emin, penalty=pen, dim=dim, max_iter=500, tol=1e-10,
                          preconditioner=pre, warm_start=False)
         out[f"pcg_{pre}_u"] = F.u.to_numpy()
         out[f"pcg_{pre}_iters"] = np.int64(n)
         # a warm-started second solve at a perturbed density
         F.rho.from_numpy(np.clip(rho * 0.9 + 0.05, 0.001, 1.0))
-        n2 = solver.solve(E_min=Emin, penalty=pen, dim=2, max_iter=500, tol=1e-10,
+        n2 = solver.solve(E_min=Emin, penalty=pen, dim=dim, max_iter=500, tol=1e-10,
                           preconditioner=pre, warm_start=True)
         out[f"pcg_{pre}_warm_u"] = F.u.to_numpy()
         out[f"pcg_{pre}_warm_iters"] = np.int64(n2)
@@ -256,6 +286,7 @@ def main():
     ref_examples = Path(ref_src).parent / "examples"
     ctx = mp.get_context("spawn")
     small = str(ref_examples / "cantilever_small.yaml")
+    cant3d = str(HERE / "yaml" / "cantilever_3d_small.yaml")
     runs = {
         "ref_run_mbb_60x20": (str(REPO / "examples" / "mbb_60x20.yaml"), {}, (1, 10, 50)),
         "ref_run_mbb_60x20_tight": (str(REPO / "examples" / "mbb_60x20.yaml"),
@@ -271,6 +302,11 @@ def main():
         "ref_run_small_earlystop": (small, {"max_iter": 200}, ()),
         "ref_run_bridge_100x50": (str(ref_examples / "bridge_2d.yaml"),
                                   {"max_iter": 12, "tol": 0.0}, (1,)),
+        "ref_run_3d_jacobi": (cant3d, {}, (1, 10)),
+        "ref_run_3d_block_jacobi": (cant3d, {"max_iter": 8,
+                                             "preconditioner": "block_jacobi"}, (1,)),
+        "ref_run_3d_sensitivity": (cant3d, {"max_iter": 8, "filter_type": "sensitivity",
+                                            "preconditioner": "none"}, (1,)),
     }
     jobs = []
     with ctx.Pool(8) as pool:
@@ -278,6 +314,8 @@ def main():
             jobs.append(("boundary", pool.apply_async(_boundary, (ref_src, ref_examples))))
         if not a.only or a.only == "ref_kernels":
             jobs.append(("ref_kernels", pool.apply_async(_kernels, (ref_src,))))
+        if not a.only or a.only == "ref_kernels3d":
+            jobs.append(("ref_kernels3d", pool.apply_async(_kernels3d, (ref_src,))))
         for name, (y, ov, snaps) in runs.items():
             if not a.only or a.only == name:
                 jobs.append((name, pool.apply_async(_run, ((ref_src, y, ov, snaps),))))

@@ -1,0 +1,297 @@
+"""GPU parity of the 3D (H8) path, called through the C ABI (tpo3_*).
+
+Checked against (a) the reference's own 3D kernels and `simp.run`, executed in
+FP64 (tests/golden/ref_kernels3d.npz, ref_run_3d_*.npz) and (b) the FP64
+oracle (oracle/simp64.py) on seeded inputs of other shapes, including
+single-element extents. Tolerances are stated per test.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import REPO, golden
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+from oracle import simp64 as O  # noqa: E402
+from toptimization_b200 import _lib  # noqa: E402
+from toptimization_b200.fem import kernels as K  # noqa: E402
+from toptimization_b200.fem.solver import PCGSolver  # noqa: E402
+from toptimization_b200.material import compute_Ke_3d, regularized_inverse  # noqa: E402
+from toptimization_b200.optimizer import filter as F  # noqa: E402
+from toptimization_b200.optimizer import oc as OCm  # noqa: E402
+from toptimization_b200.optimizer import simp  # noqa: E402
+from toptimization_b200.problem import load_problem  # noqa: E402
+
+KE3 = compute_Ke_3d(1.0, 0.3)
+G = golden("ref_kernels3d")
+DEV = "cuda"
+YAML = REPO / "tests" / "golden" / "yaml"
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _stiffness(tpo_built):
+    inv, alpha = regularized_inverse(KE3)
+    _lib.ensure_stiffness3(KE3, inv, alpha)
+
+
+def dev(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a)).to(device=DEV, dtype=dtype)
+
+
+def mask3(nn, fixed):
+    m = np.zeros(nn, dtype=np.uint8)
+    fixed = np.asarray(fixed, dtype=np.int64)
+    np.bitwise_or.at(m, fixed // 3, (1 << (fixed % 3)).astype(np.uint8))
+    return m
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def iter_band(n_ref):
+    """PCG stop points move with rounding order: the reference scatters with
+    atomics, the kernels gather in a fixed order. 2 iterations or 2 %."""
+    return max(2, round(0.02 * int(n_ref)))
+
+
+def gshape():
+    return int(G["nelx"]), int(G["nely"]), int(G["nelz"])
+
+
+def left_face(nx, ny, nz):
+    return np.arange(0, 3 * (ny + 1) * (nz + 1))
+
+
+# ---------------------------------------------------------------- matvec
+def test_matvec3_matches_reference_kernel():
+    nx, ny, nz = gshape()
+    g = _lib.grid3(nx, ny, nz, 1e-9, 3.0)
+    m = dev(mask3((nx + 1) * (ny + 1) * (nz + 1), G["fixed"]), torch.uint8)
+    ap, pap = K.matvec(g, dev(G["rho"]), m, dev(G["p"]), with_dot=True)
+    assert rel(ap.cpu().numpy(), G["Ap"]) < 1e-13
+    assert abs(pap.item() - float(G["pAp"])) <= 1e-12 * abs(float(G["pAp"]))
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(1, 1, 1), (1, 1, 6), (5, 1, 1), (1, 4, 1), (2, 3, 4),
+                                      (7, 5, 3), (16, 9, 11), (33, 17, 9)])
+def test_matvec3_vs_oracle_sizes(nx, ny, nz):
+    rng = np.random.default_rng(nx * 100 + ny * 10 + nz)
+    ne = nx * ny * nz
+    nd = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    fixed = np.unique(np.concatenate([left_face(nx, ny, nz),
+                                      rng.choice(nd, size=max(1, nd // 20), replace=False)]))
+    mesh = O.Mesh3D(nx, ny, nz, KE3, fixed)
+    rho = rng.uniform(0.001, 1.0, ne)
+    p = rng.standard_normal(nd)
+    ref = O.matvec(mesh, rho, p, 1e-9, 3.0)
+    g = _lib.grid3(nx, ny, nz, 1e-9, 3.0)
+    ap, pap = K.matvec(g, dev(rho), dev(mask3(nd // 3, fixed), torch.uint8), dev(p),
+                       with_dot=True)
+    assert rel(ap.cpu().numpy(), ref) < 1e-13
+    assert pap.item() == pytest.approx(float(p @ ref), rel=1e-12)
+
+
+# ---------------------------------------------------------------- PCG
+def _system(nx, ny, nz, fixed, loads):
+    mesh = O.Mesh3D(nx, ny, nz, KE3, fixed)
+    f = np.zeros(mesh.n_dofs)
+    for d, v in loads:
+        f[d] += v
+    f[mesh.is_fixed] = 0.0
+    return mesh, f, dev(mask3(mesh.n_nodes, fixed), torch.uint8)
+
+
+@pytest.mark.parametrize("pre", ["jacobi", "block_jacobi", "none"])
+def test_pcg3_matches_reference_solver(pre):
+    """Cold, then warm at a perturbed density, at tol 1e-10, as the
+    reference's solver.solve(dim=3) ran them."""
+    nx, ny, nz = gshape()
+    loads = list(zip(G["force_dofs"], G["force_values"]))
+    mesh, f, m = _system(nx, ny, nz, G["fixed"], loads)
+    s = PCGSolver(nx, ny, 1e-9, 3.0, float(f @ f), preconditioner=pre, max_iter=500,
+                  tol=1e-10, nelz=nz)
+    u = torch.zeros(mesh.n_dofs, dtype=torch.float64, device=DEV)
+    info = s.solve(dev(G["rho"]), dev(f), m, u, warm_start=False)
+    assert info.status == "converged"
+    assert abs(info.iters - int(G[f"pcg_{pre}_iters"])) <= iter_band(G[f"pcg_{pre}_iters"])
+    assert rel(u.cpu().numpy(), G[f"pcg_{pre}_u"]) < 1e-9
+    rho2 = np.clip(G["rho"] * 0.9 + 0.05, 0.001, 1.0)
+    info2 = s.solve(dev(rho2), dev(f), m, u, warm_start=True)
+    assert info2.status == "converged"
+    n2 = int(G[f"pcg_{pre}_warm_iters"])
+    assert abs(info2.iters - n2) <= iter_band(n2)
+    assert rel(u.cpu().numpy(), G[f"pcg_{pre}_warm_u"]) < 1e-9
+
+
+@pytest.mark.parametrize("pre", ["jacobi", "block_jacobi", "none"])
+def test_pcg3_vs_oracle_cantilever(pre):
+    """24x12x10 cantilever (left face clamped, line load on the right face),
+    random density: the same iterates as the oracle's PCG up to rounding."""
+    nx, ny, nz = 24, 12, 10
+    rng = np.random.default_rng(7)
+    rho = rng.uniform(0.05, 1.0, nx * ny * nz)
+    loads = [(3 * ((nx * (ny + 1)) * (nz + 1) + iz) + 1, -1.0 / (nz + 1)) for iz in range(nz + 1)]
+    mesh, f, m = _system(nx, ny, nz, left_face(nx, ny, nz), loads)
+    ref = O.pcg(mesh, O.simp_scale(rho, 1e-9, 3.0), f, np.zeros(mesh.n_dofs), 1e-8, 3000, pre)
+    s = PCGSolver(nx, ny, 1e-9, 3.0, float(f @ f), preconditioner=pre, max_iter=3000, tol=1e-8,
+                  nelz=nz)
+    u = torch.zeros(mesh.n_dofs, dtype=torch.float64, device=DEV)
+    info = s.solve(dev(rho), dev(f), m, u, warm_start=False)
+    assert info.status == ref.status == "converged"
+    assert abs(info.iters - ref.iters) <= iter_band(ref.iters)
+    assert rel(u.cpu().numpy(), ref.u) < 1e-6
+
+
+def test_pcg3_max_iter_and_zero_rhs():
+    nx, ny, nz = 6, 4, 3
+    mesh, f, m = _system(nx, ny, nz, left_face(nx, ny, nz), [(3 * mesh_nodes(6, 4, 3) - 2, -1.0)])
+    s = PCGSolver(nx, ny, 1e-9, 3.0, float(f @ f), max_iter=5, tol=1e-12, nelz=nz)
+    u = torch.zeros(mesh.n_dofs, dtype=torch.float64, device=DEV)
+    rho = dev(np.full(nx * ny * nz, 0.5))
+    info = s.solve(rho, dev(f), m, u, warm_start=False)
+    assert info.status == "max_iter" and info.iters == 5 and info.updates == 5
+    ref = O.pcg(mesh, O.simp_scale(np.full(nx * ny * nz, 0.5), 1e-9, 3.0), f,
+                np.zeros(mesh.n_dofs), 1e-12, 5, "jacobi")
+    assert rel(u.cpu().numpy(), ref.u) < 1e-12
+    z = PCGSolver(nx, ny, 1e-9, 3.0, 0.0, nelz=nz)
+    u.fill_(1.0)
+    info = z.solve(rho, torch.zeros_like(u), m, u, warm_start=True)
+    assert info.status == "zero_rhs" and info.iters == 0 and float(u.abs().max()) == 0.0
+
+
+def mesh_nodes(nx, ny, nz):
+    return (nx + 1) * (ny + 1) * (nz + 1)
+
+
+def test_pcg3_rejects_unsupported_forms():
+    with pytest.raises(ValueError):
+        PCGSolver(4, 3, 1e-9, 3.0, 1.0, precision="mixed", nelz=2)
+    with pytest.raises(ValueError):
+        PCGSolver(4, 3, 1e-9, 3.0, 1.0, preconditioner="nodal_block_jacobi", nelz=2)
+    # the C ABI itself refuses them too
+    g = _lib.grid3(4, 3, 2, 1e-9, 3.0)
+    cfg = _lib.TpoSolveCfg(precond=1, precision=1, max_iter=10, warm_start=0, tol=1e-8,
+                           f_norm_sq=1.0, inner_tol=1e-4, max_outer=5, poll_every=0,
+                           recurrence=0)
+    res = _lib.TpoSolveResult()
+    ws = torch.empty(1 << 20, dtype=torch.uint8, device=DEV)
+    buf = torch.zeros(3 * mesh_nodes(4, 3, 2), dtype=torch.float64, device=DEV)
+    rho = torch.full((24,), 0.5, dtype=torch.float64, device=DEV)
+    m = torch.zeros(mesh_nodes(4, 3, 2), dtype=torch.uint8, device=DEV)
+    rc = _lib.load().tpo3_pcg_solve(g, cfg, _lib.ptr(rho), _lib.ptr(buf), _lib.ptr(m),
+                                    _lib.ptr(buf), _lib.ptr(ws), ws.numel(), res,
+                                    _lib.stream_handle())
+    assert rc == 1  # TPO_ERR_ARGS
+
+
+# ---------------------------------------------------------------- sensitivity
+def test_sensitivity3_matches_reference_kernel():
+    nx, ny, nz = gshape()
+    g = _lib.grid3(nx, ny, nz, 1e-9, 3.0)
+    dc = torch.empty(nx * ny * nz, dtype=torch.float64, device=DEV)
+    c = torch.empty(1, dtype=torch.float64, device=DEV)
+    K.sensitivity(g, dev(G["rho"]), dev(G["p"]), dc, c, K.sensitivity_workspace(g, DEV))
+    assert rel(dc.cpu().numpy(), G["sens_dc"]) < 1e-13
+    assert c.item() == pytest.approx(float(G["sens_c"]), rel=1e-13)
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(1, 1, 1), (9, 2, 5), (40, 20, 20)])
+def test_sensitivity3_vs_oracle(nx, ny, nz):
+    rng = np.random.default_rng(nx + ny + nz)
+    mesh = O.Mesh3D(nx, ny, nz, KE3, np.array([0]))
+    rho = rng.uniform(0.001, 1.0, mesh.n_elem)
+    u = rng.standard_normal(mesh.n_dofs)
+    dc_ref, c_ref = O.sensitivity(mesh, u, rho, 1e-9, 3.0)
+    g = _lib.grid3(nx, ny, nz, 1e-9, 3.0)
+    dc = torch.empty(mesh.n_elem, dtype=torch.float64, device=DEV)
+    c = torch.empty(1, dtype=torch.float64, device=DEV)
+    K.sensitivity(g, dev(rho), dev(u), dc, c, K.sensitivity_workspace(g, DEV))
+    assert rel(dc.cpu().numpy(), dc_ref) < 1e-13
+    assert c.item() == pytest.approx(c_ref, rel=1e-12)
+
+
+# ---------------------------------------------------------------- filters
+@pytest.mark.parametrize("rmin", [1.5, 2.2])
+def test_filters3_match_reference_kernels(rmin):
+    nx, ny, nz = gshape()
+    g = _lib.grid3(nx, ny, nz, 1e-9, 3.0)
+    out = torch.empty(nx * ny * nz, dtype=torch.float64, device=DEV)
+    F.density_filter(g, rmin, dev(G["rho"]), out)
+    assert rel(out.cpu().numpy(), G[f"filt_rho_r{rmin}"]) < 1e-14
+    F.density_filter(g, rmin, dev(G["dc_in"]), out)
+    assert rel(out.cpu().numpy(), G[f"filt_dc_r{rmin}"]) < 1e-14
+    F.sensitivity_filter(g, rmin, dev(G["rho"]), dev(G["dc_in"]), out)
+    assert rel(out.cpu().numpy(), G[f"filt_sens_r{rmin}"]) < 1e-13
+
+
+@pytest.mark.parametrize("nx,ny,nz,rmin", [(1, 1, 1, 1.5), (13, 7, 9, 2.7), (5, 4, 3, 8.0),
+                                           (30, 20, 10, 1.0)])
+def test_filter3_vs_oracle(nx, ny, nz, rmin):
+    rng = np.random.default_rng(int(rmin * 10) + nx)
+    x = rng.uniform(0.0, 1.0, nx * ny * nz)
+    H, Hs = O.filter_matrix(nx, ny, rmin, nz)
+    g = _lib.grid3(nx, ny, nz, 1e-9, 3.0)
+    out = torch.empty(nx * ny * nz, dtype=torch.float64, device=DEV)
+    F.density_filter(g, rmin, dev(x), out)
+    assert rel(out.cpu().numpy(), O.density_filter(H, Hs, x)) < 1e-14
+
+
+def test_filter3_rejects_radius_above_limit():
+    g = _lib.grid3(4, 4, 4, 1e-9, 3.0)
+    x = torch.zeros(64, dtype=torch.float64, device=DEV)
+    with pytest.raises(_lib.TpoError):
+        F.density_filter(g, 8.5, x, torch.empty_like(x))
+
+
+# ---------------------------------------------------------------- OC
+@pytest.mark.parametrize("vf", [0.2, 0.4, 0.7])
+def test_oc3_matches_reference(vf):
+    nx, ny, nz = gshape()
+    g = _lib.grid3(nx, ny, nz, 1e-9, 3.0)
+    rho = dev(G["rho"])
+    out = torch.empty_like(rho)
+    res = torch.empty(4, dtype=torch.float64, device=DEV)
+    OCm.oc_update(g, vf, 0.2, rho, dev(G["dc_in"]), out, res, OCm.oc_workspace(g, DEV))
+    assert np.abs(out.cpu().numpy() - G[f"oc_rho_vf{vf}"]).max() < 1e-15
+    assert res[0].item() == pytest.approx(float(G[f"oc_change_vf{vf}"]), abs=1e-15)
+
+
+# ---------------------------------------------------------------- whole runs
+# The reference's 3D simp.run on the 8x4x3 cantilever. Measured spread of the
+# FP64 oracle against the same fixtures: 9.9e-11 (jacobi), 2.2e-9
+# (element-block, up to 661 CG iterations per solve), 2.3e-10 (no
+# preconditioner, sensitivity filter) in compliance; the GPU solve's
+# summation order is a third one, so the bounds are those with 10x headroom.
+@pytest.mark.parametrize("name,ov,comp_tol,rho_tol", [
+    ("3d_jacobi", {}, 1e-8, 5e-7),
+    ("3d_block_jacobi", dict(max_iter=8, preconditioner="block_jacobi"), 5e-8, 5e-7),
+    ("3d_sensitivity", dict(max_iter=8, filter_type="sensitivity", preconditioner="none"),
+     1e-8, 5e-7),
+])
+def test_run3d_matches_reference(name, ov, comp_tol, rho_tol):
+    g = golden(f"ref_run_{name}")
+    pr = load_problem(YAML / "cantilever_3d_small.yaml")
+    for k, v in ov.items():
+        setattr(pr, k, v)
+    hist = simp.RunHistory()
+    rho = simp.run(pr, live_viz=False, verbose=False, save=False, history=hist)
+    assert rho.shape == (pr.nelx, pr.nely, pr.nelz)
+    c = np.array(hist.compliance)
+    assert len(c) == len(g["compliance"])
+    assert np.max(np.abs(c - g["compliance"]) / g["compliance"]) < comp_tol
+    assert np.abs(np.array(hist.volume) - g["volume"]).max() < comp_tol
+    assert np.abs(rho.reshape(-1) - g["rho_final"]).max() < rho_tol
+    cg_ref = np.asarray(g["cg_iters"])
+    assert np.all(np.abs(np.array(hist.cg_iters) - cg_ref) <= [iter_band(n) for n in cg_ref])
+
+
+def test_run3d_rejects_unsupported_forms():
+    pr = load_problem(YAML / "cantilever_3d_small.yaml")
+    with pytest.raises(ValueError):
+        simp.run(pr, verbose=False, save=False, precision="mixed")
+    with pytest.raises(ValueError):
+        simp.run(pr, verbose=False, save=False, engine="graph", precision="mixed")

@@ -33,6 +33,12 @@ class TpoGrid(ctypes.Structure):
                 ("penalty", c_double)]
 
 
+class TpoGrid3(ctypes.Structure):
+    """3D (H8) grid: nelx x nely x nelz unit cubes."""
+    _fields_ = [("nelx", c_int32), ("nely", c_int32), ("nelz", c_int32), ("pad", c_int32),
+                ("e_min", c_double), ("penalty", c_double)]
+
+
 class TpoSolveCfg(ctypes.Structure):
     _fields_ = [("precond", c_int32), ("precision", c_int32), ("max_iter", c_int32),
                 ("warm_start", c_int32), ("tol", c_double), ("f_norm_sq", c_double),
@@ -107,6 +113,24 @@ _SIGS = {
     "tpo_profile_enable": (c_int, [c_int]),
     "tpo_profile_reset": (c_int, []),
     "tpo_profile_read": (c_int, [POINTER(TpoProfile)]),
+    "tpo_set_stiffness3": (c_int, [_PD, _PD, c_double]),
+    "tpo3_matvec_workspace_bytes": (c_size_t, [POINTER(TpoGrid3)]),
+    "tpo3_matvec_f64": (c_int, [POINTER(TpoGrid3), c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_void_p, c_size_t, c_void_p]),
+    "tpo3_pcg_workspace_bytes": (c_size_t, [POINTER(TpoGrid3), POINTER(TpoSolveCfg)]),
+    "tpo3_pcg_solve": (c_int, [POINTER(TpoGrid3), POINTER(TpoSolveCfg), c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_void_p, c_size_t, POINTER(TpoSolveResult),
+                               c_void_p]),
+    "tpo3_sensitivity_workspace_bytes": (c_size_t, [POINTER(TpoGrid3)]),
+    "tpo3_sensitivity": (c_int, [POINTER(TpoGrid3), c_void_p, c_void_p, c_void_p, c_void_p,
+                                 c_void_p, c_size_t, c_void_p]),
+    "tpo3_density_filter": (c_int, [POINTER(TpoGrid3), c_double, c_void_p, c_void_p,
+                                    c_void_p]),
+    "tpo3_sensitivity_filter": (c_int, [POINTER(TpoGrid3), c_double, c_void_p, c_void_p,
+                                        c_void_p, c_void_p]),
+    "tpo3_oc_workspace_bytes": (c_size_t, [POINTER(TpoGrid3)]),
+    "tpo3_oc_update": (c_int, [POINTER(TpoGrid3), c_double, c_double, c_void_p, c_void_p,
+                               c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "tpo_batch_workspace_bytes": (c_size_t, [c_int32]),
     "tpo_batch_design_workspace_bytes": (c_size_t, [POINTER(TpoBatchDesign),
                                                     POINTER(TpoBatchLayout)]),
@@ -159,6 +183,14 @@ def grid(nelx: int, nely: int, e_min: float, penalty: float) -> TpoGrid:
     return TpoGrid(int(nelx), int(nely), float(e_min), float(penalty))
 
 
+def grid3(nelx: int, nely: int, nelz: int, e_min: float, penalty: float) -> TpoGrid3:
+    return TpoGrid3(int(nelx), int(nely), int(nelz), 0, float(e_min), float(penalty))
+
+
+def is3d(g) -> bool:
+    return isinstance(g, TpoGrid3)
+
+
 def ptr(t) -> int:
     """Device pointer of a torch tensor (0 for None)."""
     return 0 if t is None else int(t.data_ptr())
@@ -189,13 +221,33 @@ def ensure_stiffness(Ke, Ke_inv, alpha_reg: float) -> None:
     _stiffness_set[dev] = key
 
 
+def ensure_stiffness3(Ke, Ke_inv, alpha_reg: float) -> None:
+    """Upload the 24x24 H8 Ke and its regularised inverse, once per device
+    and matrix."""
+    import numpy as np
+    import torch
+    dev = torch.cuda.current_device()
+    ke = np.ascontiguousarray(Ke, dtype=np.float64).reshape(576)
+    ki = np.ascontiguousarray(Ke_inv, dtype=np.float64).reshape(576)
+    key = ke.tobytes() + ki.tobytes() + np.float64(alpha_reg).tobytes()
+    if _stiffness3_set.get(dev) == key:
+        return
+    check(load().tpo_set_stiffness3(ke.ctypes.data_as(_PD), ki.ctypes.data_as(_PD),
+                                    c_double(alpha_reg)))
+    _stiffness3_set[dev] = key
+
+
+_stiffness3_set: dict[int, bytes] = {}
+
+
 def profile_read() -> dict:
     p = TpoProfile()
     check(load().tpo_profile_read(p))
     return {k: getattr(p, k) for k, _ in TpoProfile._fields_}
 
 
-__all__ = ["load", "check", "grid", "ptr", "stream_handle", "ensure_stiffness", "TpoGrid",
+__all__ = ["load", "check", "grid", "grid3", "is3d", "ptr", "stream_handle",
+           "ensure_stiffness", "ensure_stiffness3", "TpoGrid", "TpoGrid3",
            "TpoSolveCfg", "TpoSolveResult", "TpoBatchCfg", "TpoBatchDesign", "TpoBatchLayout",
            "TpoError", "PRECOND", "PRECISION", "SOLVE_STATUS",
            "exported_symbols", "c_float", "c_uint8"]

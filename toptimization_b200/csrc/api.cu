@@ -19,6 +19,7 @@
 #include "design.cuh"
 #include "pcg.cuh"
 #include "cgstep.cuh"
+#include "hex3d.cuh"
 #include "stencil.cuh"
 #include "tpo.h"
 
@@ -1275,3 +1276,6 @@ int tpo_oc_update(const tpo_grid *g, double volfrac, double move, const double *
 
 // batched designs (tpo_batch_*): host side, same translation unit
 #include "batch_host.cuh"
+
+// 3D (H8) designs (tpo3_*): host side, same translation unit
+#include "hex3d_host.cuh"

@@ -1,0 +1,487 @@
+// 3D path: trilinear hexahedra (H8) on a structured nelx x nely x nelz grid of
+// unit cubes. Reference: fem/kernels.py:104-129 (diagonal), :179-212
+// (matvec), :275-308 (sensitivity); fem/fused_kernels.py:59-94 (matvec + p.Ap);
+// fem/preconditioner.py:34-44,112-156 (element-block preconditioner);
+// optimizer/filter.py:75-97 (3D filter box).
+//
+// Layouts are the reference's numbering (mesh.py:68-112), used as they are:
+//   node (ix, iy, iz)    -> (ix*(nely+1) + iy)*(nelz+1) + iz    (iz fastest)
+//   nodal vector v       -> v[3*node + {0:x, 1:y, 2:z}]
+//   element (ex, ey, ez) -> (ex*nely + ey)*nelz + ez
+//   fixed mask           -> uint8 per node, bit0/1/2 = x/y/z fixed
+//
+// Every nodal operator is a gather: one thread per node sums the rows of its
+// (up to) eight elements. Thread n reads the 27-node neighbourhood once (3
+// values each) and keeps one partial 3-vector per incident element,
+//   y_k += Ke[3a+c][3b+j] v_m[j]      (a: the node's corner in element k,
+//                                       b: neighbour m's corner),
+// then scales each by its element weight: 64 node pairs x 9 multiply-adds +
+// 24 = 600 FP64 FMAs per node, no atomics, a fixed summation order. All
+// corner indices are compile-time constants after unrolling, so every Ke entry
+// is a constant-bank operand. At these arithmetic intensities the FP64 pipe,
+// not HBM, is the bound (576 FMAs against ~57 bytes per node).
+#pragma once
+
+#include "common.cuh"
+
+namespace tpo {
+
+// 24x24 H8 stiffness and its regularised inverse (element-block
+// preconditioner), row-major, DOFs [x,y,z] per corner in mesh.py:87-96 order.
+__constant__ double c_ke3[576];
+__constant__ double c_kinv3[576];
+
+constexpr int H3_THREADS = 128;  // gather kernels
+constexpr int H3_FLAT = 256;     // pointwise kernels
+constexpr int H3_MAXR = 8;       // filter: ceil(rmin) <= 8
+
+struct Hex3 {
+  int nx, ny, nz;  // elements per axis
+  __host__ __device__ int64_t nodes() const { return (int64_t)(nx + 1) * (ny + 1) * (nz + 1); }
+  __host__ __device__ int64_t elems() const { return (int64_t)nx * ny * nz; }
+};
+
+// H8 corner index of offset (dx, dy, dz) in {0,1}^3: bottom face (z = 0)
+// counter-clockwise from (0,0), then the top face (reference mesh.py:87-96).
+__host__ __device__ constexpr int h8_corner(int dx, int dy, int dz) {
+  return 4 * dz + (dy ? (dx ? 2 : 3) : (dx ? 1 : 0));
+}
+
+template <bool INV> __device__ __forceinline__ double kent3(int i);
+template <> __device__ __forceinline__ double kent3<false>(int i) { return c_ke3[i]; }
+template <> __device__ __forceinline__ double kent3<true>(int i) { return c_kinv3[i]; }
+
+struct NodePos {
+  int ix, iy, iz;
+  int64_t n;
+};
+
+__device__ __forceinline__ NodePos node_pos(const Hex3 &g, int64_t n) {
+  NodePos p;
+  p.n = n;
+  const int64_t nz1 = g.nz + 1, ny1 = g.ny + 1;
+  const int64_t col = n / nz1;
+  p.iz = (int)(n - col * nz1);
+  p.ix = (int)(col / ny1);
+  p.iy = (int)(col - (int64_t)p.ix * ny1);
+  return p;
+}
+
+// Element weights around a node: k = (ex*2 + ey)*2 + ez for the element with
+// origin (ix-1+ex, iy-1+ey, iz-1+ez); 0 outside the grid.
+__device__ __forceinline__ void node_elem_weights(const Hex3 &g, const NodePos &p,
+                                                  const double *__restrict__ w, double (&we)[8]) {
+#pragma unroll
+  for (int ex = 0; ex < 2; ++ex)
+#pragma unroll
+    for (int ey = 0; ey < 2; ++ey)
+#pragma unroll
+      for (int ez = 0; ez < 2; ++ez) {
+        const int x = p.ix - 1 + ex, y = p.iy - 1 + ey, z = p.iz - 1 + ez;
+        const bool ok = x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz;
+        we[(ex * 2 + ey) * 2 + ez] = ok ? w[((int64_t)x * g.ny + y) * g.nz + z] : 0.0;
+      }
+}
+
+// 1/sqrt(number of elements at a node) (elements sharing each of its DOFs,
+// reference preconditioner.py:34-44): the count is a product of three
+// factors 1 or 2, so the root is one of four constants.
+__device__ __forceinline__ double inv_sqrt_count(const Hex3 &g, int ix, int iy, int iz) {
+  const int k = (ix > 0 && ix < g.nx) + (iy > 0 && iy < g.ny) + (iz > 0 && iz < g.nz);
+  return k == 0 ? 1.0 : k == 1 ? 0.70710678118654752440 : k == 2 ? 0.5 : 0.35355339059327376220;
+}
+
+// out[c] = sum_k we[k] sum_{b,j} M[3a_k+c][3b+j] v(b)[j] over the node's 8
+// elements; load(ox, oy, oz, v) returns neighbour (ix+ox, iy+oy, iz+oz)'s three
+// values (zeros outside the grid).
+template <bool INV, typename Load>
+__device__ __forceinline__ void hex_gather(const double (&we)[8], Load load, double (&out)[3]) {
+  double y[8][3];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) y[k][0] = y[k][1] = y[k][2] = 0.0;
+#pragma unroll
+  for (int ox = -1; ox <= 1; ++ox)
+#pragma unroll
+    for (int oy = -1; oy <= 1; ++oy)
+#pragma unroll
+      for (int oz = -1; oz <= 1; ++oz) {
+        double v[3];
+        load(ox, oy, oz, v);
+#pragma unroll
+        for (int ex = 0; ex < 2; ++ex)
+#pragma unroll
+          for (int ey = 0; ey < 2; ++ey)
+#pragma unroll
+            for (int ez = 0; ez < 2; ++ez) {
+              const int bx = ox + 1 - ex, by = oy + 1 - ey, bz = oz + 1 - ez;
+              if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+              const int a = h8_corner(1 - ex, 1 - ey, 1 - ez);
+              const int b = h8_corner(bx, by, bz);
+              const int k = (ex * 2 + ey) * 2 + ez;
+#pragma unroll
+              for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                  y[k][c] = fma(kent3<INV>((3 * a + c) * 24 + 3 * b + j), v[j], y[k][c]);
+            }
+      }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t = fma(we[k], y[k][c], t);
+    out[c] = t;
+  }
+}
+
+// in-grid neighbour test and its flat node index
+struct Nbr {
+  const Hex3 &g;
+  const NodePos &p;
+  int64_t sx, sy;  // node strides along x, y
+  __device__ __forceinline__ bool at(int ox, int oy, int oz, int64_t &m) const {
+    const int x = p.ix + ox, y = p.iy + oy, z = p.iz + oz;
+    m = p.n + ox * sx + oy * sy + oz;
+    return x >= 0 && x <= g.nx && y >= 0 && y <= g.ny && z >= 0 && z <= g.nz;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Gather kernels
+// ---------------------------------------------------------------------------
+enum Hex3Mode {
+  H3_APPLY = 0,  // ap = K p (fixed rows: p), p.ap
+  H3_RES = 1,    // r = f - K u, z = r / diag (or r), r.z, ||r||^2: first residual
+  H3_DIR = 2,    // p' = z + beta p (p' = z first), ap = K p', p'.ap -> alpha
+  H3_BLOCK = 3   // z = element-block M r, r.z, ||r||^2 -> stop / beta
+};
+
+struct Hex3Args {
+  Hex3 g;
+  const double *w;       // element weights: SIMP scales (block: s / max(s, alpha)^2)
+  const uint8_t *mask;
+  const double *x;       // APPLY: p; RES: u; DIR: z; BLOCK: r
+  double *pa, *pb;       // DIR: direction ping-pong pair (by the parity of ctl->it)
+  const double *f;       // RES: load
+  const double *diag;    // RES: Jacobi diagonal (nullptr: no preconditioner)
+  double *out;           // APPLY/DIR: ap; RES: r; BLOCK: z
+  double *z;             // RES: z (Jacobi)
+  double *part;
+  PcgCtl *ctl;           // RES/DIR/BLOCK
+  uint32_t *counter;     // APPLY
+  double *pap_out;       // APPLY (nullable)
+  int init;              // BLOCK: first residual of the solve
+};
+
+template <int MODE, int PRE>
+__global__ void __launch_bounds__(H3_THREADS) k_hex_gather(Hex3Args a) {
+  PcgCtl *ctl = a.ctl;
+  if (MODE != H3_APPLY && ctl->status != TPO_SOLVE_RUNNING) return;
+  const Hex3 g = a.g;
+  const int64_t total = g.nodes();
+  const int64_t sy = g.nz + 1, sx = (int64_t)(g.ny + 1) * sy;
+  bool first = true;
+  double beta = 0.0;
+  const double *pold = nullptr;
+  double *pnew = nullptr;
+  if (MODE == H3_DIR) {
+    first = ctl->first != 0;
+    beta = ctl->beta;
+    // iteration k reads the direction of k-1 and writes its own into the other
+    // buffer; the update kernel of iteration k reads it from there
+    const bool odd = ctl->it & 1;
+    pold = odd ? a.pb : a.pa;
+    pnew = odd ? a.pa : a.pb;
+  }
+  double acc[2] = {0.0, 0.0};
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < total;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const NodePos p = node_pos(g, n);
+    const Nbr nb{g, p, sx, sy};
+    double we[8];
+    node_elem_weights(g, p, a.w, we);
+    double own[3] = {0.0, 0.0, 0.0};  // this node's input values (direction: p')
+    double o[3];
+    auto load = [&](int ox, int oy, int oz, double (&v)[3]) {
+      int64_t m;
+      const bool ok = nb.at(ox, oy, oz, m);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) v[j] = 0.0;
+      if (ok) {
+        const double *src = a.x + 3 * m;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) v[j] = src[j];
+        if (MODE == H3_DIR && !first) {
+          const double *po = pold + 3 * m;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) v[j] = fma(beta, po[j], v[j]);
+        }
+        if (MODE == H3_BLOCK) {
+          const double s = inv_sqrt_count(g, p.ix + ox, p.iy + oy, p.iz + oz);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) v[j] *= s;
+        }
+      }
+      if (ox == 0 && oy == 0 && oz == 0) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) own[j] = v[j];
+      }
+    };
+    hex_gather<MODE == H3_BLOCK>(we, load, o);
+    const unsigned fm = a.mask[n];
+    double *dst = a.out + 3 * n;
+    if (MODE == H3_APPLY || MODE == H3_DIR) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double ap = ((fm >> c) & 1u) ? own[c] : o[c];
+        dst[c] = ap;
+        acc[0] = fma(own[c], ap, acc[0]);
+      }
+      if (MODE == H3_DIR) {
+        double *pn = pnew + 3 * n;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) pn[c] = own[c];
+      }
+    } else if (MODE == H3_RES) {
+      // fixed rows of K are identity rows: (K u)_fixed = u_fixed
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double ku = ((fm >> c) & 1u) ? own[c] : o[c];
+        const double r = a.f[3 * n + c] - ku;
+        dst[c] = r;
+        double z = r;
+        if (PRE == TPO_PRECOND_JACOBI) {
+          z = r / a.diag[3 * n + c];
+          a.z[3 * n + c] = z;
+        }
+        acc[0] = fma(r, z, acc[0]);
+        acc[1] = fma(r, r, acc[1]);
+      }
+    } else {  // H3_BLOCK
+      const double s = inv_sqrt_count(g, p.ix, p.iy, p.iz);
+      const double *r = a.x + 3 * n;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double z = ((fm >> c) & 1u) ? 0.0 : o[c] * s;
+        dst[c] = z;
+        acc[0] = fma(r[c], z, acc[0]);
+        acc[1] = fma(r[c], r[c], acc[1]);
+      }
+    }
+  }
+  uint32_t *counter = MODE == H3_APPLY ? a.counter : &ctl->counter;
+  if (!grid_reduce<2>(acc, a.part, counter)) return;
+  if (threadIdx.x != 0) return;
+  if (MODE == H3_APPLY) {
+    if (a.pap_out) *a.pap_out = acc[0];
+  } else if (MODE == H3_DIR) {
+    const double pap = acc[0];
+    ctl->pap = pap;
+    ctl->first = 0;
+    if (!finite(pap)) ctl->status = TPO_SOLVE_NONFINITE;
+    else if (fabs(pap) < 1e-30) ctl->status = TPO_SOLVE_BREAKDOWN;  // solver.py:114-115
+    else ctl->alpha = ctl->rz / pap;                                  // solver.py:117
+  } else if (MODE == H3_RES || a.init) {
+    ctl->it = 0;
+    ctl->first = 1;
+    ctl->rz = acc[0];
+    ctl->rr = acc[1];
+    if (!finite(acc[0]) || !finite(acc[1])) ctl->status = TPO_SOLVE_NONFINITE;
+  } else {
+    finish_update(ctl, acc[0], acc[1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pointwise kernels
+// ---------------------------------------------------------------------------
+// u += alpha p', r -= alpha ap; Jacobi / none: z = r / diag (or r), r.z,
+// ||r||^2 and the stop / beta decision. Element-block: u and r only (the
+// preconditioner kernel that follows reduces and decides).
+template <int PRE>
+__global__ void __launch_bounds__(H3_FLAT)
+    k_hex_update(int64_t ndof, double *__restrict__ u, double *__restrict__ r,
+                 const double *__restrict__ pa, const double *__restrict__ pb,
+                 const double *__restrict__ ap, const double *__restrict__ diag,
+                 double *__restrict__ z, double *part, PcgCtl *ctl) {
+  if (ctl->status != TPO_SOLVE_RUNNING) return;
+  const double alpha = ctl->alpha;
+  const double *__restrict__ p = (ctl->it & 1) ? pa : pb;  // written by this iteration's direction
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ndof;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    u[i] = fma(alpha, p[i], u[i]);
+    const double rn = fma(-alpha, ap[i], r[i]);
+    r[i] = rn;
+    if (PRE != TPO_PRECOND_BLOCK_JACOBI) {
+      double zn = rn;
+      if (PRE == TPO_PRECOND_JACOBI) {
+        zn = rn / diag[i];
+        z[i] = zn;
+      }
+      acc[0] = fma(rn, zn, acc[0]);
+      acc[1] = fma(rn, rn, acc[1]);
+    }
+  }
+  if (PRE == TPO_PRECOND_BLOCK_JACOBI) return;
+  if (!grid_reduce<2>(acc, part, &ctl->counter)) return;
+  if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
+}
+
+// SIMP scales s = e_min + rho^p (1 - e_min) (reference fem/kernels.py:92) and,
+// for the element-block preconditioner, w = s / max(s, alpha)^2
+// (preconditioner.py:128-130).
+__global__ void k_hex_scales(int64_t ne, const double *__restrict__ rho, double e_min, double pen,
+                             double alpha_reg, double *__restrict__ s, double *__restrict__ w) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const double v = e_min + pow(rho[e], pen) * (1.0 - e_min);
+    s[e] = v;
+    if (w) {
+      const double sc = fmax(v, alpha_reg);
+      w[e] = v / (sc * sc);
+    }
+  }
+}
+
+// Jacobi diagonal: sum_e s_e Ke_ii over the node's elements; fixed -> 1,
+// floor 1e-20 (reference fem/kernels.py:104-129).
+__global__ void k_hex_diag(Hex3 g, const double *__restrict__ s, const uint8_t *__restrict__ mask,
+                           double *__restrict__ diag) {
+  const int64_t total = g.nodes();
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < total;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const NodePos p = node_pos(g, n);
+    double we[8];
+    node_elem_weights(g, p, s, we);
+    const unsigned fm = mask[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double d = 0.0;
+#pragma unroll
+      for (int ex = 0; ex < 2; ++ex)
+#pragma unroll
+        for (int ey = 0; ey < 2; ++ey)
+#pragma unroll
+          for (int ez = 0; ez < 2; ++ez) {
+            const int a = h8_corner(1 - ex, 1 - ey, 1 - ez);
+            d = fma(we[(ex * 2 + ey) * 2 + ez], c_ke3[(3 * a + c) * 25], d);
+          }
+      if ((fm >> c) & 1u) d = 1.0;
+      else if (d < 1e-20) d = 1e-20;
+      diag[3 * n + c] = d;
+    }
+  }
+}
+
+// Warm start: fixed DOFs of u are zeroed (reference solver.py:52-57).
+__global__ void k_hex_zero_fixed(int64_t nn, const uint8_t *__restrict__ mask, double *u) {
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned fm = mask[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      if ((fm >> c) & 1u) u[3 * n + c] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Compliance and sensitivity, one element per thread (reference
+// fem/kernels.py:275-308): uKu_e = u_e^T Ke u_e, dc_e = -p rho^(p-1)(1-e_min) uKu_e,
+// c = sum_e (e_min + rho^p (1 - e_min)) uKu_e.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(H3_THREADS)
+    k_hex_sensitivity(Hex3 g, double e_min, double pen, const double *__restrict__ rho,
+                      const double *__restrict__ u, double *__restrict__ dc, double *part,
+                      SumCtl *ctl, double *c_out) {
+  const int64_t ne = g.elems();
+  const int64_t sy = g.nz + 1, sx = (int64_t)(g.ny + 1) * sy;
+  double acc[1] = {0.0};
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t col = e / g.nz;
+    const int ez = (int)(e - col * g.nz);
+    const int ex = (int)(col / g.ny);
+    const int ey = (int)(col - (int64_t)ex * g.ny);
+    const int64_t n0 = (int64_t)ex * sx + (int64_t)ey * sy + ez;
+    double ue[24];
+#pragma unroll
+    for (int dx = 0; dx < 2; ++dx)
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+        for (int dz = 0; dz < 2; ++dz) {
+          const int b = h8_corner(dx, dy, dz);
+          const double *src = u + 3 * (n0 + dx * sx + dy * sy + dz);
+#pragma unroll
+          for (int j = 0; j < 3; ++j) ue[3 * b + j] = src[j];
+        }
+    double uku = 0.0;
+#pragma unroll
+    for (int i = 0; i < 24; ++i) {
+      double ku = c_ke3[i * 24] * ue[0];
+#pragma unroll
+      for (int j = 1; j < 24; ++j) ku = fma(c_ke3[i * 24 + j], ue[j], ku);
+      uku = fma(ue[i], ku, uku);
+    }
+    const double r = rho[e];
+    dc[e] = -pen * pow(r, pen - 1.0) * (1.0 - e_min) * uku;
+    acc[0] += (e_min + pow(r, pen) * (1.0 - e_min)) * uku;
+  }
+  if (!grid_reduce<1>(acc, part, &ctl->counter)) return;
+  if (threadIdx.x == 0) *c_out = acc[0];
+}
+
+// ---------------------------------------------------------------------------
+// Hat-weight filters over the 3D box |dx|,|dy|,|dz| <= R = ceil(rmin)
+// (reference optimizer/filter.py:75-97,106-171): the weights
+// w = rmin - sqrt(dx^2+dy^2+dz^2) of the box are derived once per CTA into
+// shared memory; neighbours are summed in the reference's order (dx outer,
+// dz inner), skipping w <= 0 and out-of-domain elements.
+//   density: out = sum w x_j / (sum w + 1e-20)
+//   sens:    out = sum w rho_j dc_j / (rho_e sum w + 1e-20)
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(H3_FLAT)
+    k_hex_filter(Hex3 g, double rmin, int R, const double *__restrict__ x,
+                 const double *__restrict__ rho, double *__restrict__ out) {
+  extern __shared__ double hw[];
+  const int W = 2 * R + 1;
+  for (int k = threadIdx.x; k < W * W * W; k += blockDim.x) {
+    const int dx = k / (W * W) - R, dy = (k / W) % W - R, dz = k % W - R;
+    hw[k] = rmin - sqrt((double)(dx * dx + dy * dy + dz * dz));
+  }
+  __syncthreads();
+  const int64_t ne = g.elems();
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t col = e / g.nz;
+    const int ez = (int)(e - col * g.nz);
+    const int ex = (int)(col / g.ny);
+    const int ey = (int)(col - (int64_t)ex * g.ny);
+    double num = 0.0, den = 0.0;
+    for (int dx = -R; dx <= R; ++dx) {
+      const int jx = ex + dx;
+      if (jx < 0 || jx >= g.nx) continue;
+      for (int dy = -R; dy <= R; ++dy) {
+        const int jy = ey + dy;
+        if (jy < 0 || jy >= g.ny) continue;
+        const double *wrow = hw + ((dx + R) * W + (dy + R)) * W + R;
+        const int64_t jbase = ((int64_t)jx * g.ny + jy) * g.nz;
+        for (int dz = -R; dz <= R; ++dz) {
+          const int jz = ez + dz;
+          const double w = wrow[dz];
+          if (w > 0.0 && jz >= 0 && jz < g.nz) {
+            const int64_t j = jbase + jz;
+            const double v = (MODE == F_SENS) ? rho[j] * x[j] : x[j];
+            num = fma(w, v, num);
+            den += w;
+          }
+        }
+      }
+    }
+    out[e] = (MODE == F_SENS) ? num / (rho[e] * den + 1e-20) : num / (den + 1e-20);
+  }
+}
+
+}  // namespace tpo

@@ -1,0 +1,381 @@
+// libtpo: host side of the 3D (H8) entry points, tpo3_* in include/tpo.h.
+// Included at the end of api.cu (same translation unit: the error, launch
+// and polling helpers and the __constant__ stiffness are shared).
+#pragma once
+
+namespace {
+
+bool g_have_stiffness3[kMaxDevices];
+double g_alpha_reg3[kMaxDevices];
+
+// Launch-size caps: grid-stride loops cover larger grids, and the grid
+// reductions read at most this many partials.
+constexpr int kHexMaxCtas = 2048;
+
+int check_grid3(const tpo_grid3 *g) {
+  if (!g) return fail(TPO_ERR_ARGS, "grid is NULL");
+  if (g->nelx < 1 || g->nely < 1 || g->nelz < 1)
+    return fail(TPO_ERR_ARGS, "nelx, nely, nelz must be >= 1");
+  if ((int64_t)(g->nelx + 1) * (g->nely + 1) * (g->nelz + 1) > ((int64_t)1 << 30))
+    return fail(TPO_ERR_ARGS, "grid too large");
+  return TPO_OK;
+}
+
+int need_stiffness3(int *dev) {
+  int rc = current_device(dev);
+  if (rc) return rc;
+  if (!g_have_stiffness3[*dev])
+    return fail(TPO_ERR_NO_STIFFNESS, "tpo_set_stiffness3 has not been called on device %d",
+                *dev);
+  return TPO_OK;
+}
+
+Hex3 hex_of(const tpo_grid3 *g) { return Hex3{g->nelx, g->nely, g->nelz}; }
+dim3 hex_gather_grid(const Hex3 &h) { return flat_grid(h.nodes(), H3_THREADS, kHexMaxCtas); }
+dim3 hex_elem_grid(const Hex3 &h) { return flat_grid(h.elems(), H3_THREADS, kHexMaxCtas); }
+dim3 hex_flat_grid(int64_t n) { return flat_grid(n, H3_FLAT, kHexMaxCtas); }
+
+struct Pcg3Ws {
+  PcgCtl *ctl;
+  double *s, *w, *diag, *r, *z, *pa, *pb, *ap, *part;
+  size_t bytes;
+};
+
+Pcg3Ws carve_pcg3(void *base, const tpo_grid3 *g, const tpo_solve_cfg *c) {
+  const Hex3 h = hex_of(g);
+  const size_t ne = h.elems(), nd = 3 * h.nodes();
+  Carve cv(base);
+  Pcg3Ws w{};
+  w.ctl = cv.take<PcgCtl>(1);
+  w.s = cv.take<double>(ne);
+  if (c->precond == TPO_PRECOND_BLOCK_JACOBI) w.w = cv.take<double>(ne);
+  if (c->precond == TPO_PRECOND_JACOBI) w.diag = cv.take<double>(nd);
+  w.r = cv.take<double>(nd);
+  if (c->precond != TPO_PRECOND_NONE) w.z = cv.take<double>(nd);
+  w.pa = cv.take<double>(nd);
+  w.pb = cv.take<double>(nd);
+  w.ap = cv.take<double>(nd);
+  w.part = cv.take<double>(2 * (size_t)kHexMaxCtas);
+  w.bytes = cv.off;
+  return w;
+}
+
+template <int PRE>
+int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const double *f,
+         const uint8_t *fixed, double *u, const Pcg3Ws &w, tpo_solve_result *out,
+         cudaStream_t st, double alpha_reg) {
+  const Hex3 h = hex_of(g);
+  const int64_t nn = h.nodes(), nd = 3 * nn, ne = h.elems();
+  const double fn = std::sqrt(c->f_norm_sq);
+  const double tol_sq = (c->tol * fn) * (c->tol * fn);
+  const dim3 gg = hex_gather_grid(h), fg = hex_flat_grid(nd);
+  // warm start from u with its fixed DOFs zeroed, else from zero (solver.py:52-57)
+  if (c->warm_start) {
+    k_hex_zero_fixed<<<hex_flat_grid(nn), H3_FLAT, 0, st>>>(nn, fixed, u);
+    TPO_CK_LAUNCH();
+  } else {
+    TPO_CK(cudaMemsetAsync(u, 0, nd * sizeof(double), st));
+  }
+  k_hex_scales<<<hex_flat_grid(ne), H3_FLAT, 0, st>>>(ne, rho, g->e_min, g->penalty, alpha_reg,
+                                                      w.s, w.w);
+  TPO_CK_LAUNCH();
+  if (PRE == TPO_PRECOND_JACOBI) {
+    k_hex_diag<<<gg, H3_THREADS, 0, st>>>(h, w.s, fixed, w.diag);
+    TPO_CK_LAUNCH();
+  }
+  k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, 0.0, c->max_iter, nullptr, 0.0, 0);
+  TPO_CK_LAUNCH();
+
+  Hex3Args a{};
+  a.g = h;
+  a.w = w.s;
+  a.mask = fixed;
+  a.part = w.part;
+  a.ctl = w.ctl;
+  // r = f - K u, z = M r (point preconditioners), r.z, ||r||^2
+  a.x = u;
+  a.f = f;
+  a.diag = w.diag;
+  a.out = w.r;
+  a.z = w.z;
+  k_hex_gather<H3_RES, PRE><<<gg, H3_THREADS, 0, st>>>(a);
+  TPO_CK_LAUNCH();
+  Hex3Args b{};  // element-block z = M r
+  b.g = h;
+  b.w = w.w;
+  b.mask = fixed;
+  b.x = w.r;
+  b.out = w.z;
+  b.part = w.part;
+  b.ctl = w.ctl;
+  if (PRE == TPO_PRECOND_BLOCK_JACOBI) {
+    b.init = 1;
+    k_hex_gather<H3_BLOCK, 0><<<gg, H3_THREADS, 0, st>>>(b);
+    TPO_CK_LAUNCH();
+    b.init = 0;
+  }
+  Hex3Args d{};  // p' = z + beta p, ap = K p', alpha
+  d.g = h;
+  d.w = w.s;
+  d.mask = fixed;
+  d.x = PRE == TPO_PRECOND_NONE ? w.r : w.z;
+  d.pa = w.pa;
+  d.pb = w.pb;
+  d.out = w.ap;
+  d.part = w.part;
+  d.ctl = w.ctl;
+
+  auto iter = [&](cudaEvent_t *ev) -> int {
+    if (ev) TPO_CK(cudaEventRecord(ev[0], st));
+    k_hex_gather<H3_DIR, 0><<<gg, H3_THREADS, 0, st>>>(d);
+    TPO_CK_LAUNCH();
+    if (ev) TPO_CK(cudaEventRecord(ev[1], st));
+    if (ev) TPO_CK(cudaEventRecord(ev[2], st));
+    k_hex_update<PRE><<<fg, H3_FLAT, 0, st>>>(nd, u, w.r, w.pa, w.pb, w.ap, w.diag, w.z, w.part,
+                                              w.ctl);
+    TPO_CK_LAUNCH();
+    if (PRE == TPO_PRECOND_BLOCK_JACOBI) {
+      k_hex_gather<H3_BLOCK, 0><<<gg, H3_THREADS, 0, st>>>(b);
+      TPO_CK_LAUNCH();
+    }
+    if (ev) TPO_CK(cudaEventRecord(ev[3], st));
+    return TPO_OK;
+  };
+  // algorithmic bytes: direction z|r, p_old -> p', ap; scales; mask. Update:
+  // u, r, p', ap -> u, r (+ diag -> z); element-block: r -> z, weights, mask.
+  LaunchBytes lb{};
+  lb.dir = 4 * nd * 8 + ne * 8 + nn;
+  lb.update = 6 * nd * 8 + (PRE == TPO_PRECOND_JACOBI ? 2 * nd * 8 : 0) +
+              (PRE == TPO_PRECOND_BLOCK_JACOBI ? 2 * nd * 8 + ne * 8 + nn : 0);
+  PcgCtl fin;
+  const int chunk = c->poll_every > 0 ? c->poll_every : 16;
+  int rc = run_iterations(iter, w.ctl, c->max_iter, 0, chunk, st, &fin, lb);
+  if (rc) return rc;
+  int status = fin.status;
+  if (status == TPO_SOLVE_RUNNING) status = TPO_SOLVE_MAX_ITER;  // max_iter <= 0
+  out->status = status;
+  out->updates = fin.it;
+  out->iters = (status == TPO_SOLVE_CONVERGED) ? fin.it : c->max_iter;
+  out->outer_iters = 1;
+  out->rr = fin.rr;
+  return TPO_OK;
+}
+
+struct Sens3Ws {
+  SumCtl *ctl;
+  double *part;
+  size_t bytes;
+};
+Sens3Ws carve_sens3(void *base) {
+  Carve cv(base);
+  Sens3Ws w{};
+  w.ctl = cv.take<SumCtl>(1);
+  w.part = cv.take<double>(2 * (size_t)kHexMaxCtas);
+  w.bytes = cv.off;
+  return w;
+}
+
+int filter3_launch(const tpo_grid3 *g, double rmin, int mode, const double *x, const double *rho,
+                   double *out, tpo_stream s) {
+  int rc = check_grid3(g);
+  if (rc) return rc;
+  if (!x || !out || (mode == F_SENS && !rho)) return fail(TPO_ERR_ARGS, "NULL pointer argument");
+  if (!(rmin > 0.0)) return fail(TPO_ERR_ARGS, "rmin must be > 0");
+  const int R = (int)std::ceil(rmin);
+  if (R > H3_MAXR) return fail(TPO_ERR_ARGS, "ceil(rmin) = %d > %d", R, H3_MAXR);
+  const int W = 2 * R + 1;
+  const size_t smem = (size_t)W * W * W * sizeof(double);
+  const Hex3 h = hex_of(g);
+  cudaStream_t st = static_cast<cudaStream_t>(s);
+  const dim3 gr = hex_flat_grid(h.elems());
+  if (mode == F_SENS)
+    k_hex_filter<F_SENS><<<gr, H3_FLAT, smem, st>>>(h, rmin, R, x, rho, out);
+  else
+    k_hex_filter<F_DENSITY><<<gr, H3_FLAT, smem, st>>>(h, rmin, R, x, nullptr, out);
+  TPO_CK_LAUNCH();
+  return TPO_OK;
+}
+
+// The OC bisection is pointwise over elements: the 3D design runs through the
+// same kernels as a 2D grid of E x 1 elements.
+tpo_grid flat_oc_grid(const tpo_grid3 *g) {
+  tpo_grid f{};
+  f.nelx = (int32_t)hex_of(g).elems();
+  f.nely = 1;
+  f.e_min = g->e_min;
+  f.penalty = g->penalty;
+  return f;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tpo_set_stiffness3(const double ke[576], const double ke_inv[576], double alpha_reg) {
+  if (!ke || !ke_inv) return fail(TPO_ERR_ARGS, "ke and ke_inv must be non-NULL");
+  int dev;
+  int rc = current_device(&dev);
+  if (rc) return rc;
+  for (int i = 0; i < 576; ++i)
+    if (!std::isfinite(ke[i]) || !std::isfinite(ke_inv[i]))
+      return fail(TPO_ERR_ARGS, "non-finite stiffness entry %d", i);
+  TPO_CK(cudaMemcpyToSymbol(c_ke3, ke, sizeof(double) * 576));
+  TPO_CK(cudaMemcpyToSymbol(c_kinv3, ke_inv, sizeof(double) * 576));
+  g_alpha_reg3[dev] = alpha_reg;
+  g_have_stiffness3[dev] = true;
+  return TPO_OK;
+}
+
+size_t tpo3_matvec_workspace_bytes(const tpo_grid3 *g) {
+  if (check_grid3(g)) return 0;
+  Carve cv(nullptr);
+  cv.take<SumCtl>(1);
+  cv.take<double>(2 * (size_t)kHexMaxCtas);
+  cv.take<double>((size_t)hex_of(g).elems());
+  return cv.off;
+}
+
+int tpo3_matvec_f64(const tpo_grid3 *g, const double *rho, const uint8_t *fixed, const double *p,
+                    double *ap, double *pap_out, void *ws, size_t ws_bytes, tpo_stream s) {
+  int rc = check_grid3(g);
+  if (rc) return rc;
+  int dev;
+  if ((rc = need_stiffness3(&dev))) return rc;
+  if (!rho || !fixed || !p || !ap || !ws) return fail(TPO_ERR_ARGS, "NULL pointer argument");
+  if (!aligned(p, 8) || !aligned(ap, 8) || !aligned(ws, kAlign))
+    return fail(TPO_ERR_ARGS, "misaligned pointer");
+  if (ws_bytes < tpo3_matvec_workspace_bytes(g))
+    return fail(TPO_ERR_WORKSPACE, "workspace too small");
+  const Hex3 h = hex_of(g);
+  cudaStream_t st = static_cast<cudaStream_t>(s);
+  Carve cv(ws);
+  SumCtl *ctl = cv.take<SumCtl>(1);
+  double *part = cv.take<double>(2 * (size_t)kHexMaxCtas);
+  double *sc = cv.take<double>((size_t)h.elems());
+  TPO_CK(cudaMemsetAsync(ctl, 0, sizeof(SumCtl), st));
+  k_hex_scales<<<hex_flat_grid(h.elems()), H3_FLAT, 0, st>>>(h.elems(), rho, g->e_min,
+                                                             g->penalty, 0.0, sc, nullptr);
+  TPO_CK_LAUNCH();
+  Hex3Args a{};
+  a.g = h;
+  a.w = sc;
+  a.mask = fixed;
+  a.x = p;
+  a.out = ap;
+  a.part = part;
+  a.counter = &ctl->counter;
+  a.pap_out = pap_out;
+  cudaEvent_t *ev = nullptr;
+  if (g_prof_on && (rc = prof_events(1, &ev))) return rc;
+  if (ev) TPO_CK(cudaEventRecord(ev[0], st));
+  k_hex_gather<H3_APPLY, 0><<<hex_gather_grid(h), H3_THREADS, 0, st>>>(a);
+  TPO_CK_LAUNCH();
+  if (ev) {
+    TPO_CK(cudaEventRecord(ev[1], st));
+    TPO_CK(cudaEventSynchronize(ev[1]));
+    float ms = 0.f;
+    TPO_CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    g_prof.apply_launches += 1;
+    g_prof.apply_ms += ms;
+    g_prof.apply_bytes += 2 * 3 * h.nodes() * 8 + h.elems() * 8 + h.nodes();
+  }
+  return TPO_OK;
+}
+
+size_t tpo3_pcg_workspace_bytes(const tpo_grid3 *g, const tpo_solve_cfg *c) {
+  if (check_grid3(g) || !c) return 0;
+  return carve_pcg3(nullptr, g, c).bytes;
+}
+
+int tpo3_pcg_solve(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho_phys,
+                   const double *f, const uint8_t *fixed, double *u, void *ws, size_t ws_bytes,
+                   tpo_solve_result *out, tpo_stream s) {
+  int rc = check_grid3(g);
+  if (rc) return rc;
+  if (!c || !out) return fail(TPO_ERR_ARGS, "cfg and result must be non-NULL");
+  int dev;
+  if ((rc = need_stiffness3(&dev))) return rc;
+  if (!rho_phys || !f || !fixed || !u || !ws) return fail(TPO_ERR_ARGS, "NULL pointer argument");
+  if (!aligned(f, 8) || !aligned(u, 8) || !aligned(ws, kAlign))
+    return fail(TPO_ERR_ARGS, "misaligned pointer (vectors need 8 B, workspace 256 B)");
+  if (c->precond != TPO_PRECOND_NONE && c->precond != TPO_PRECOND_JACOBI &&
+      c->precond != TPO_PRECOND_BLOCK_JACOBI)
+    return fail(TPO_ERR_ARGS, "3D solves take none, jacobi or block_jacobi (got %d)", c->precond);
+  if (c->precision != TPO_PRECISION_FP64)
+    return fail(TPO_ERR_ARGS, "3D solves are FP64 only");
+  if (c->recurrence != TPO_RECURRENCE_AUTO && c->recurrence != TPO_RECURRENCE_STANDARD)
+    return fail(TPO_ERR_ARGS, "3D solves use the standard recurrence");
+  if (!(c->tol >= 0.0) || !(c->f_norm_sq >= 0.0))
+    return fail(TPO_ERR_ARGS, "tol and f_norm_sq must be >= 0");
+  const Pcg3Ws w = carve_pcg3(ws, g, c);
+  if (ws_bytes < w.bytes) return fail(TPO_ERR_WORKSPACE, "workspace %zu < %zu", ws_bytes, w.bytes);
+  cudaStream_t st = static_cast<cudaStream_t>(s);
+  memset(out, 0, sizeof(*out));
+  if (std::sqrt(c->f_norm_sq) < 1e-30) {  // reference solver.py:59-63
+    TPO_CK(cudaMemsetAsync(u, 0, 3 * hex_of(g).nodes() * sizeof(double), st));
+    TPO_CK(cudaStreamSynchronize(st));
+    out->status = TPO_SOLVE_ZERO_RHS;
+    return TPO_OK;
+  }
+  const double ar = g_alpha_reg3[dev];
+  switch (c->precond) {
+    case TPO_PRECOND_NONE:
+      return pcg3<TPO_PRECOND_NONE>(g, c, rho_phys, f, fixed, u, w, out, st, ar);
+    case TPO_PRECOND_JACOBI:
+      return pcg3<TPO_PRECOND_JACOBI>(g, c, rho_phys, f, fixed, u, w, out, st, ar);
+    default:
+      return pcg3<TPO_PRECOND_BLOCK_JACOBI>(g, c, rho_phys, f, fixed, u, w, out, st, ar);
+  }
+}
+
+size_t tpo3_sensitivity_workspace_bytes(const tpo_grid3 *g) {
+  if (check_grid3(g)) return 0;
+  return carve_sens3(nullptr).bytes;
+}
+
+int tpo3_sensitivity(const tpo_grid3 *g, const double *rho_phys, const double *u, double *dc,
+                     double *compliance_out, void *ws, size_t ws_bytes, tpo_stream s) {
+  int rc = check_grid3(g);
+  if (rc) return rc;
+  int dev;
+  if ((rc = need_stiffness3(&dev))) return rc;
+  if (!rho_phys || !u || !dc || !compliance_out || !ws)
+    return fail(TPO_ERR_ARGS, "NULL pointer argument");
+  if (!aligned(ws, kAlign)) return fail(TPO_ERR_ARGS, "misaligned workspace");
+  const Sens3Ws w = carve_sens3(ws);
+  if (ws_bytes < w.bytes) return fail(TPO_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t st = static_cast<cudaStream_t>(s);
+  TPO_CK(cudaMemsetAsync(w.ctl, 0, sizeof(SumCtl), st));
+  const Hex3 h = hex_of(g);
+  k_hex_sensitivity<<<hex_elem_grid(h), H3_THREADS, 0, st>>>(h, g->e_min, g->penalty, rho_phys,
+                                                            u, dc, w.part, w.ctl, compliance_out);
+  TPO_CK_LAUNCH();
+  return TPO_OK;
+}
+
+int tpo3_density_filter(const tpo_grid3 *g, double rmin, const double *x, double *out,
+                        tpo_stream s) {
+  return filter3_launch(g, rmin, F_DENSITY, x, nullptr, out, s);
+}
+
+int tpo3_sensitivity_filter(const tpo_grid3 *g, double rmin, const double *rho, const double *dc,
+                            double *out, tpo_stream s) {
+  return filter3_launch(g, rmin, F_SENS, dc, rho, out, s);
+}
+
+size_t tpo3_oc_workspace_bytes(const tpo_grid3 *g) {
+  if (check_grid3(g)) return 0;
+  const tpo_grid f = flat_oc_grid(g);
+  return tpo_oc_workspace_bytes(&f);
+}
+
+int tpo3_oc_update(const tpo_grid3 *g, double volfrac, double move, const double *rho_in,
+                   const double *dc, const double *dv, double *rho_out, double *result_out,
+                   void *ws, size_t ws_bytes, tpo_stream s) {
+  int rc = check_grid3(g);
+  if (rc) return rc;
+  const tpo_grid f = flat_oc_grid(g);
+  return tpo_oc_update(&f, volfrac, move, rho_in, dc, dv, rho_out, result_out, ws, ws_bytes, s);
+}
+
+}  // extern "C"

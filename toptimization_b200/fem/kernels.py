@@ -4,6 +4,10 @@ Counterparts of the reference's `src/toptimization/fem/kernels.py`:
   matvec        -> compute_matvec_2d / matvec_and_dot_2d   (kernels.py:143-176,
                    fused_kernels.py:21-56)
   sensitivity   -> compute_sensitivity_2d                   (kernels.py:234-272)
+With a `TpoGrid3` (3D, H8) the same calls run compute_matvec_3d /
+matvec_and_dot_3d (kernels.py:179-212, fused_kernels.py:59-94) and
+compute_sensitivity_3d (kernels.py:275-308), FP64 only; the reference
+dispatches on `dim` the same way.
 All arguments are CUDA tensors; calls are asynchronous on the current stream.
 """
 
@@ -32,10 +36,14 @@ def matvec(grid: _lib.TpoGrid, rho: torch.Tensor, fixed: torch.Tensor, p: torch.
     if ap is None:
         ap = torch.empty_like(p)
     if workspace is None:
-        workspace = torch.empty(lib.tpo_matvec_workspace_bytes(grid), dtype=torch.uint8,
-                                device=p.device)
+        workspace = matvec_workspace(grid, p.device)
     pap = torch.empty(1, dtype=torch.float64, device=p.device) if with_dot else None
-    fn = lib.tpo_matvec_f64 if p.dtype == torch.float64 else lib.tpo_matvec_f32
+    if _lib.is3d(grid):
+        if p.dtype != torch.float64:
+            raise ValueError("the 3D matvec is FP64 only")
+        fn = lib.tpo3_matvec_f64
+    else:
+        fn = lib.tpo_matvec_f64 if p.dtype == torch.float64 else lib.tpo_matvec_f32
     if rho.dtype != p.dtype:
         raise ValueError("rho and p must share a dtype")
     _lib.check(fn(grid, _lib.ptr(rho), _lib.ptr(fixed), _lib.ptr(p), _lib.ptr(ap),
@@ -55,8 +63,10 @@ def apply_stiffness(grid: _lib.TpoGrid, scale: torch.Tensor, fixed: torch.Tensor
                   _lib.ptr(pap), _lib.ptr(workspace), workspace.numel(), _lib.stream_handle()))
 
 
-def matvec_workspace(grid: _lib.TpoGrid, device) -> torch.Tensor:
-    n = _lib.load().tpo_matvec_workspace_bytes(grid)
+def matvec_workspace(grid, device) -> torch.Tensor:
+    lib = _lib.load()
+    n = (lib.tpo3_matvec_workspace_bytes(grid) if _lib.is3d(grid)
+         else lib.tpo_matvec_workspace_bytes(grid))
     return torch.empty(n, dtype=torch.uint8, device=device)
 
 
@@ -65,11 +75,14 @@ def sensitivity(grid: _lib.TpoGrid, rho_phys: torch.Tensor, u: torch.Tensor,
     """dc = d(compliance)/d(rho_phys); compliance[0] = sum_e scale_e u_e^T Ke u_e."""
     _require_cuda(rho_phys, u, dc, compliance, workspace)
     lib = _lib.load()
-    _lib.check(lib.tpo_sensitivity(grid, _lib.ptr(rho_phys), _lib.ptr(u), _lib.ptr(dc),
+    fn = lib.tpo3_sensitivity if _lib.is3d(grid) else lib.tpo_sensitivity
+    _lib.check(fn(grid, _lib.ptr(rho_phys), _lib.ptr(u), _lib.ptr(dc),
                                    _lib.ptr(compliance), _lib.ptr(workspace), workspace.numel(),
                                    _lib.stream_handle()))
 
 
-def sensitivity_workspace(grid: _lib.TpoGrid, device) -> torch.Tensor:
-    n = _lib.load().tpo_sensitivity_workspace_bytes(grid)
+def sensitivity_workspace(grid, device) -> torch.Tensor:
+    lib = _lib.load()
+    n = (lib.tpo3_sensitivity_workspace_bytes(grid) if _lib.is3d(grid)
+         else lib.tpo_sensitivity_workspace_bytes(grid))
     return torch.empty(n, dtype=torch.uint8, device=device)

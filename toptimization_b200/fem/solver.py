@@ -21,6 +21,8 @@ preconditioner; the element-block preconditioner and the mixed form keep two),
 "standard" (the reference's own recurrence, two launches per iteration) or
 "single" (force the one-launch form). The two recurrences produce the same
 iterates in exact arithmetic.
+3D (H8) grids (`nelz` > 0) solve in FP64 with "jacobi", "block_jacobi" or
+"none" and the standard recurrence (`tpo3_pcg_solve`), the same rules.
 Precisions: "fp64" (plain) and "mixed" (Krylov vectors r, p, Ap stored in
 FP32, FP64 arithmetic, dot products, alpha/beta and solution u; the recursive
 residual is replaced by the FP64 residual f - K u whenever it has dropped by
@@ -59,7 +61,7 @@ class PCGSolver:
                  f_norm_sq: float, *, preconditioner: str = "jacobi",
                  precision: str = "fp64", max_iter: int = 2000, tol: float = 1e-8,
                  inner_tol: float = 1e-4, max_outer: int = 50, poll_every: int = 0,
-                 recurrence: str = "auto", device=None):
+                 recurrence: str = "auto", device=None, nelz: int = 0):
         if preconditioner not in _lib.PRECOND:
             raise ValueError(f"unknown preconditioner {preconditioner!r}")
         if precision not in _lib.PRECISION:
@@ -69,15 +71,23 @@ class PCGSolver:
         if recurrence == "single" and (preconditioner == "block_jacobi" or precision != "fp64"):
             raise ValueError("the one-launch recurrence serves the FP64 solve with a point "
                              "preconditioner only")
+        if nelz and (preconditioner == "nodal_block_jacobi" or precision != "fp64"
+                     or recurrence == "single"):
+            raise ValueError("3D solves are FP64 with jacobi, block_jacobi or none and the "
+                             "standard recurrence")
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
-        self.grid = _lib.grid(nelx, nely, e_min, penalty)
+        self.grid = (_lib.grid3(nelx, nely, nelz, e_min, penalty) if nelz
+                     else _lib.grid(nelx, nely, e_min, penalty))
         self.cfg = _lib.TpoSolveCfg(
             precond=_lib.PRECOND[preconditioner], precision=_lib.PRECISION[precision],
             max_iter=int(max_iter), warm_start=1, tol=float(tol), f_norm_sq=float(f_norm_sq),
             inner_tol=float(inner_tol), max_outer=int(max_outer), poll_every=int(poll_every),
             recurrence=RECURRENCE[recurrence])
-        nbytes = _lib.load().tpo_pcg_workspace_bytes(self.grid, self.cfg)
+        lib = _lib.load()
+        self._solve = lib.tpo3_pcg_solve if nelz else lib.tpo_pcg_solve
+        nbytes = (lib.tpo3_pcg_workspace_bytes(self.grid, self.cfg) if nelz
+                  else lib.tpo_pcg_workspace_bytes(self.grid, self.cfg))
         self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
 
     def solve(self, rho_phys: torch.Tensor, f: torch.Tensor, fixed: torch.Tensor,
@@ -91,7 +101,7 @@ class PCGSolver:
             raise ValueError("fixed must be a uint8 per-node mask")
         self.cfg.warm_start = 1 if warm_start else 0
         res = _lib.TpoSolveResult()
-        _lib.check(_lib.load().tpo_pcg_solve(
+        _lib.check(self._solve(
             self.grid, self.cfg, _lib.ptr(rho_phys), _lib.ptr(f), _lib.ptr(fixed), _lib.ptr(u),
             _lib.ptr(self.workspace), self.workspace.numel(), res, _lib.stream_handle()))
         return SolveInfo(_lib.SOLVE_STATUS.get(res.status, str(res.status)), res.iters,

@@ -24,6 +24,7 @@ H8_CORNERS = ((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0),
 
 FIXED_X = 1  # bit in the per-node fixed mask
 FIXED_Y = 2
+FIXED_Z = 4
 
 
 def build_edof_2d(problem) -> np.ndarray:
@@ -75,11 +76,11 @@ def element_centers(problem) -> np.ndarray:
 
 
 # --------------------------------------------------------------------------
-# Device-side layouts (2D)
+# Per-node arrays the device reads (2D and 3D)
 # --------------------------------------------------------------------------
 
 def fixed_node_mask(problem) -> np.ndarray:
-    """uint8 per node: bit0 = x DOF fixed, bit1 = y DOF fixed.
+    """uint8 per node: bit0 = x DOF fixed, bit1 = y DOF fixed (3D: bit2 = z).
 
     Replaces the reference's int32-per-DOF `is_fixed` field
     (`src/toptimization/fem/fields.py:146-148`) with one byte per node.
@@ -87,8 +88,8 @@ def fixed_node_mask(problem) -> np.ndarray:
     mask = np.zeros(problem.n_nodes, dtype=np.uint8)
     dofs = np.asarray(problem.fixed_dofs, dtype=np.int64)
     if dofs.size:
-        np.bitwise_or.at(mask, dofs // 2, np.where(dofs % 2 == 0, FIXED_X, FIXED_Y)
-                         .astype(np.uint8))
+        dim = problem.dim
+        np.bitwise_or.at(mask, dofs // dim, (1 << (dofs % dim)).astype(np.uint8))
     return mask
 
 

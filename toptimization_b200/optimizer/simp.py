@@ -16,6 +16,10 @@ Per OC iteration (`simp.py:141-219`):
 simp.py:174-189). Every field lives in one `SimpDesign` as CUDA tensors; the
 host reads five scalars per iteration.
 
+3D problems (dim 3, H8 elements) run the same loop through the tpo3_* entry
+points: FP64 PCG with "jacobi", "block_jacobi" or "none", the 3D filter box,
+and the result shaped (nelx, nely, nelz) (`simp.py:309-312`).
+
 Not reproduced: Taichi backend selection (CUDA only), matplotlib live
 windows and PNG output (headless; `density_final.npy` and the histories are
 written as in `simp.py:294-306`).
@@ -36,7 +40,7 @@ import torch
 from .. import _lib
 from ..fem import kernels as K
 from ..fem.solver import PCGSolver, SolveInfo
-from ..material import compute_Ke_2d, regularized_inverse
+from ..material import compute_Ke_2d, compute_Ke_3d, regularized_inverse
 from ..mesh import fixed_node_mask, force_vector
 from . import filter as filt
 from . import oc as oc_mod
@@ -78,8 +82,6 @@ class SimpDesign:
 
     def __init__(self, problem, device=None, precision: str | None = None,
                  preconditioner: str | None = None, poll_every: int = 0):
-        if problem.dim != 2:
-            raise NotImplementedError("toptimization_b200 implements the 2D Q4 path only")
         self.problem = pr = problem
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
@@ -87,11 +89,20 @@ class SimpDesign:
             raise ValueError("SimpDesign needs a CUDA device")
         self.precision = precision or getattr(pr, "precision", "fp64")
         self.preconditioner = preconditioner or pr.preconditioner
+        nelz = pr.nelz if pr.dim == 3 else 0
+        if nelz and self.precision != "fp64":
+            raise ValueError("3D designs run the FP64 solve")
         with torch.cuda.device(self.device):
-            Ke = compute_Ke_2d(pr.E, pr.nu)
-            Ke_inv, alpha = regularized_inverse(Ke)
-            _lib.ensure_stiffness(Ke, Ke_inv, alpha)
-        self.grid = _lib.grid(pr.nelx, pr.nely, pr.E_min, pr.penalty)
+            if nelz:
+                Ke = compute_Ke_3d(pr.E, pr.nu)
+                Ke_inv, alpha = regularized_inverse(Ke)
+                _lib.ensure_stiffness3(Ke, Ke_inv, alpha)
+            else:
+                Ke = compute_Ke_2d(pr.E, pr.nu)
+                Ke_inv, alpha = regularized_inverse(Ke)
+                _lib.ensure_stiffness(Ke, Ke_inv, alpha)
+        self.grid = (_lib.grid3(pr.nelx, pr.nely, nelz, pr.E_min, pr.penalty) if nelz
+                     else _lib.grid(pr.nelx, pr.nely, pr.E_min, pr.penalty))
         dev = self.device
         f_np = force_vector(pr)
         self.f_norm_sq = float(np.dot(f_np, f_np))
@@ -111,7 +122,7 @@ class SimpDesign:
                                 inner_tol=getattr(pr, "inner_tol", 1e-4),
                                 max_outer=getattr(pr, "max_outer_iter", 50),
                                 recurrence=getattr(pr, "recurrence", "auto"),
-                                poll_every=poll_every, device=dev)
+                                poll_every=poll_every, device=dev, nelz=nelz)
         self.sens_ws = K.sensitivity_workspace(self.grid, dev)
         self.oc_ws = oc_mod.oc_workspace(self.grid, dev)
         self.it = 0
@@ -197,7 +208,8 @@ def run(problem, backend: str = "auto", live_viz: bool = True,
         save: bool = True, history: RunHistory | None = None,
         engine: str = "direct") -> np.ndarray:
     """Run SIMP topology optimisation; returns the final design density as an
-    array of shape (nelx, nely), FP64 (reference simp.py:19-41,309-312).
+    array of shape (nelx, nely) -- (nelx, nely, nelz) in 3D -- FP64 (reference
+    simp.py:19-41,309-312).
 
     `viz_callback(rho_np, it, compliance, volume)` is called every iteration
     (simp.py:213-214). `live_viz` is accepted for compatibility; there is no
@@ -208,9 +220,9 @@ def run(problem, backend: str = "auto", live_viz: bool = True,
     """
     _check_backend(backend)
     pr = problem
-    if pr.dim != 2:
-        raise NotImplementedError("toptimization_b200 implements the 2D Q4 path only")
     if engine == "graph":
+        if pr.dim != 2:
+            raise ValueError("engine='graph' runs 2D designs")
         if (precision or pr.precision) != "mixed":
             raise ValueError("engine='graph' runs the mixed-precision form")
         design = GraphDesign(pr, device=device, preconditioner=preconditioner)
@@ -221,7 +233,8 @@ def run(problem, backend: str = "auto", live_viz: bool = True,
         raise ValueError(f"unknown engine {engine!r}")
     hist = history if history is not None else RunHistory()
     if verbose:
-        print(f"[toptimization_b200] {pr.name}: {pr.nelx}x{pr.nely}, n_dofs={pr.n_dofs:,}, "
+        size = f"{pr.nelx}x{pr.nely}" + (f"x{pr.nelz}" if pr.dim == 3 else "")
+        print(f"[toptimization_b200] {pr.name}: {size}, n_dofs={pr.n_dofs:,}, "
               f"precision={design.precision}, preconditioner={design.preconditioner}")
         print(f"{'Iter':>5} {'Compliance':>14} {'Volume':>8} {'Change':>9} {'CG':>6} {'s/iter':>7}")
         print("-" * 55)
@@ -240,6 +253,8 @@ def run(problem, backend: str = "auto", live_viz: bool = True,
     rho = design.density()
     if save:
         _save_final(pr, rho, hist)
+    if pr.dim == 3:
+        return rho.reshape(pr.nelx, pr.nely, pr.nelz)
     return rho.reshape(pr.nelx, pr.nely)
 
 
