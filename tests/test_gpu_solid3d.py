@@ -76,8 +76,13 @@ def test_matvec3_matches_reference_kernel():
     assert abs(pap.item() - float(G["pAp"])) <= 1e-12 * abs(float(G["pAp"]))
 
 
+# Launch forms covered: the plane-marching kernel with one plane per CTA
+# chunk (small grids), with two planes per chunk (699x2x3, 200x25x25; the
+# latter also has a partial last CTA per plane), and the per-node kernel
+# (nelz = 1350, 1400: the plane staging would exceed shared memory).
 @pytest.mark.parametrize("nx,ny,nz", [(1, 1, 1), (1, 1, 6), (5, 1, 1), (1, 4, 1), (2, 3, 4),
-                                      (7, 5, 3), (16, 9, 11), (33, 17, 9)])
+                                      (7, 5, 3), (16, 9, 11), (33, 17, 9), (699, 2, 3),
+                                      (200, 25, 25), (1, 1, 1400), (2, 1, 1350)])
 def test_matvec3_vs_oracle_sizes(nx, ny, nz):
     rng = np.random.default_rng(nx * 100 + ny * 10 + nz)
     ne = nx * ny * nz
@@ -87,7 +92,7 @@ def test_matvec3_vs_oracle_sizes(nx, ny, nz):
     mesh = O.Mesh3D(nx, ny, nz, KE3, fixed)
     rho = rng.uniform(0.001, 1.0, ne)
     p = rng.standard_normal(nd)
-    ref = O.matvec(mesh, rho, p, 1e-9, 3.0)
+    ref = O.matvec_free(mesh, O.simp_scale(rho, 1e-9, 3.0), p)
     g = _lib.grid3(nx, ny, nz, 1e-9, 3.0)
     ap, pap = K.matvec(g, dev(rho), dev(mask3(nd // 3, fixed), torch.uint8), dev(p),
                        with_dot=True)
@@ -144,6 +149,32 @@ def test_pcg3_vs_oracle_cantilever(pre):
     assert info.status == ref.status == "converged"
     assert abs(info.iters - ref.iters) <= iter_band(ref.iters)
     assert rel(u.cpu().numpy(), ref.u) < 1e-6
+
+
+@pytest.mark.parametrize("pre", ["jacobi", "block_jacobi", "none"])
+def test_pcg3_per_node_kernel_path(pre):
+    """A 3x2x1300 column (front face clamped, load on the back face): nelz is
+    too large for the plane staging, so every gather runs the per-node kernel.
+    Exactly 200 iterations (unconverged) against the oracle's 200."""
+    nx, ny, nz = 3, 2, 1300
+    rng = np.random.default_rng(11)
+    rho = rng.uniform(0.05, 1.0, nx * ny * nz)
+    nodes = np.arange(mesh_nodes(nx, ny, nz))
+    iz = nodes % (nz + 1)
+    fixed = np.sort(np.concatenate([3 * nodes[iz == 0] + c for c in range(3)]))
+    loads = [(3 * n + 1, -0.1) for n in nodes[iz == nz]]
+    mesh, f, m = _system(nx, ny, nz, fixed, loads)
+    ref = O.pcg(mesh, O.simp_scale(rho, 1e-9, 3.0), f, np.zeros(mesh.n_dofs), 1e-14, 200, pre,
+                assemble=False)
+    assert ref.status == "max_iter"
+    s = PCGSolver(nx, ny, 1e-9, 3.0, float(f @ f), preconditioner=pre, max_iter=200, tol=1e-14,
+                  nelz=nz)
+    u = torch.zeros(mesh.n_dofs, dtype=torch.float64, device=DEV)
+    info = s.solve(dev(rho), dev(f), m, u, warm_start=False)
+    assert info.status == "max_iter" and info.updates == 200
+    # 200 unconverged steps amplify rounding differences; a wrong index
+    # would give O(1) differences
+    assert rel(u.cpu().numpy(), ref.u) < 1e-7
 
 
 def test_pcg3_max_iter_and_zero_rhs():
@@ -266,13 +297,16 @@ def test_oc3_matches_reference(vf):
 # (element-block, up to 661 CG iterations per solve), 2.3e-10 (no
 # preconditioner, sensitivity filter) in compliance; the GPU solve's
 # summation order is a third one, so the bounds are those with 10x headroom.
-@pytest.mark.parametrize("name,ov,comp_tol,rho_tol", [
-    ("3d_jacobi", {}, 1e-8, 5e-7),
-    ("3d_block_jacobi", dict(max_iter=8, preconditioner="block_jacobi"), 5e-8, 5e-7),
+# The element-block solves have lost orthogonality long before they stop, so
+# their stop points move with rounding: measured on B200 up to 14 of 570
+# iterations (2.5 %) against the reference, 12 (2 %) for the oracle.
+@pytest.mark.parametrize("name,ov,comp_tol,rho_tol,cg_rel", [
+    ("3d_jacobi", {}, 1e-8, 5e-7, 0.02),
+    ("3d_block_jacobi", dict(max_iter=8, preconditioner="block_jacobi"), 5e-8, 5e-7, 0.04),
     ("3d_sensitivity", dict(max_iter=8, filter_type="sensitivity", preconditioner="none"),
-     1e-8, 5e-7),
+     1e-8, 5e-7, 0.02),
 ])
-def test_run3d_matches_reference(name, ov, comp_tol, rho_tol):
+def test_run3d_matches_reference(name, ov, comp_tol, rho_tol, cg_rel):
     g = golden(f"ref_run_{name}")
     pr = load_problem(YAML / "cantilever_3d_small.yaml")
     for k, v in ov.items():
@@ -286,7 +320,7 @@ def test_run3d_matches_reference(name, ov, comp_tol, rho_tol):
     assert np.abs(np.array(hist.volume) - g["volume"]).max() < comp_tol
     assert np.abs(rho.reshape(-1) - g["rho_final"]).max() < rho_tol
     cg_ref = np.asarray(g["cg_iters"])
-    assert np.all(np.abs(np.array(hist.cg_iters) - cg_ref) <= [iter_band(n) for n in cg_ref])
+    assert np.all(np.abs(np.array(hist.cg_iters) - cg_ref) <= np.maximum(2, cg_rel * cg_ref))
 
 
 def test_run3d_rejects_unsupported_forms():

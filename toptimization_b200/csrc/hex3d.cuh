@@ -293,6 +293,201 @@ __global__ void __launch_bounds__(H3_THREADS) k_hex_gather(Hex3Args a) {
 }
 
 // ---------------------------------------------------------------------------
+// Plane-marching form of the same gathers. A CTA owns HT_THREADS consecutive
+// nodes j0 .. j0+T-1 of a y-z plane (plane index j = iy*(nelz+1) + iz, one
+// node per thread) and walks them along x over a chunk of planes. Node
+// values (direction: p' = z + beta p, formed ONCE per node) are staged per
+// plane in shared memory for the run j0-(nelz+2) .. j0+T+nelz+1, which holds
+// every y/z neighbour of the CTA's nodes, in a ring of three planes (x-1, x,
+// x+1); element weights in a ring of two element planes. Global loads are
+// contiguous runs of each plane; the 27-point gather reads shared memory.
+// Neighbours that wrap around a z-row are never used with a nonzero weight:
+// every element containing them lies outside the grid, and those weights are
+// zero. Layout of the dynamic shared memory (doubles):
+//   nodes  [3 planes][3 components][NH],  NH = T + 2*(nelz+2)
+//   elems  [2 planes][EH],                EH = T + nelz + 2
+// ---------------------------------------------------------------------------
+constexpr int HT_THREADS = 256;
+
+__host__ __device__ inline int hex_tile_nh(int nz) { return HT_THREADS + 2 * (nz + 2); }
+__host__ __device__ inline int hex_tile_eh(int nz) { return HT_THREADS + nz + 2; }
+__host__ __device__ inline size_t hex_tile_smem(int nz) {
+  return (size_t)(9 * hex_tile_nh(nz) + 2 * hex_tile_eh(nz)) * sizeof(double);
+}
+
+template <int MODE, int PRE>
+__global__ void __launch_bounds__(HT_THREADS) k_hex_tile(Hex3Args a, int xc) {
+  PcgCtl *ctl = a.ctl;
+  if (MODE != H3_APPLY && ctl->status != TPO_SOLVE_RUNNING) return;
+  extern __shared__ double hs[];
+  const Hex3 g = a.g;
+  const int nz1 = g.nz + 1;
+  const int64_t P = (int64_t)(g.ny + 1) * nz1;  // nodes per x-plane
+  const int64_t PE = (int64_t)g.ny * g.nz;      // elements per x-plane
+  const int NH = hex_tile_nh(g.nz), EH = hex_tile_eh(g.nz);
+  double *sv = hs;            // node ring
+  double *se = hs + 9 * NH;   // element ring
+  const int64_t j0 = (int64_t)blockIdx.x * HT_THREADS;
+  const int xa = blockIdx.y * xc, xb = min(xa + xc, g.nx + 1);
+  const int64_t j = j0 + threadIdx.x;
+  const bool mine = j < P;
+  const int iy = (int)(j / nz1), iz = (int)(j - (int64_t)iy * nz1);
+  const int iy0 = (int)(j0 / nz1), iz0 = (int)(j0 - (int64_t)iy0 * nz1);
+  const int64_t kmin = (int64_t)(iy0 - 1) * g.nz + (iz0 - 1);  // first staged element
+  const int hoff = g.nz + 2;                                  // halo before j0
+
+  bool first = true;
+  double beta = 0.0;
+  const double *pold = nullptr;
+  double *pnew = nullptr;
+  if (MODE == H3_DIR) {
+    first = ctl->first != 0;
+    beta = ctl->beta;
+    const bool odd = ctl->it & 1;
+    pold = odd ? a.pb : a.pa;
+    pnew = odd ? a.pa : a.pb;
+  }
+
+  auto load_nodes = [&](int x, int slot) {
+    double *d = sv + slot * 3 * NH;
+    for (int i = threadIdx.x; i < NH; i += HT_THREADS) {
+      const int64_t jj = j0 - hoff + i;
+      double v[3] = {0.0, 0.0, 0.0};
+      if (x >= 0 && x <= g.nx && jj >= 0 && jj < P) {
+        const int64_t m = (int64_t)x * P + jj;
+        const double *src = a.x + 3 * m;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = src[c];
+        if (MODE == H3_DIR) {
+          if (!first) {
+            const double *po = pold + 3 * m;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c] = fma(beta, po[c], v[c]);
+          }
+          // the CTA's own nodes: store the new direction once
+          if (x >= xa && x < xb && i >= hoff && i < hoff + HT_THREADS) {
+            double *pn = pnew + 3 * m;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) pn[c] = v[c];
+          }
+        }
+        if (MODE == H3_BLOCK) {
+          const int my = (int)(jj / nz1), mz = (int)(jj - (int64_t)my * nz1);
+          const double s = inv_sqrt_count(g, x, my, mz);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) v[c] *= s;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) d[c * NH + i] = v[c];
+    }
+  };
+  auto load_elems = [&](int ex, int slot) {
+    double *d = se + slot * EH;
+    for (int i = threadIdx.x; i < EH; i += HT_THREADS) {
+      const int64_t k = kmin + i;
+      d[i] = (ex >= 0 && ex < g.nx && k >= 0 && k < PE) ? a.w[(int64_t)ex * PE + k] : 0.0;
+    }
+  };
+
+  load_nodes(xa - 1, (xa + 2) % 3);
+  load_nodes(xa, xa % 3);
+  load_elems(xa - 1, (xa + 1) % 2);
+  double acc[2] = {0.0, 0.0};
+  const int c0 = (int)(j - j0) + hoff;  // this node's slot in a staged plane
+  for (int x = xa; x < xb; ++x) {
+    load_nodes(x + 1, (x + 1) % 3);
+    load_elems(x, x % 2);
+    __syncthreads();
+    if (mine) {
+      const double *pl[3] = {sv + ((x + 2) % 3) * 3 * NH, sv + (x % 3) * 3 * NH,
+                             sv + ((x + 1) % 3) * 3 * NH};
+      const double *el[2] = {se + ((x + 1) % 2) * EH, se + (x % 2) * EH};
+      double we[8];
+#pragma unroll
+      for (int ex = 0; ex < 2; ++ex)
+#pragma unroll
+        for (int ey = 0; ey < 2; ++ey)
+#pragma unroll
+          for (int ez = 0; ez < 2; ++ez) {
+            const int y = iy - 1 + ey, z = iz - 1 + ez;
+            const bool ok = y >= 0 && y < g.ny && z >= 0 && z < g.nz;
+            we[(ex * 2 + ey) * 2 + ez] = ok ? el[ex][(int64_t)y * g.nz + z - kmin] : 0.0;
+          }
+      double own[3] = {0.0, 0.0, 0.0};
+      auto load = [&](int ox, int oy, int oz, double (&v)[3]) {
+        const double *src = pl[ox + 1] + c0 + oy * nz1 + oz;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = src[c * NH];
+        if (ox == 0 && oy == 0 && oz == 0) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) own[c] = v[c];
+        }
+      };
+      double o[3];
+      hex_gather<MODE == H3_BLOCK>(we, load, o);
+      const int64_t n = (int64_t)x * P + j;
+      const unsigned fm = a.mask[n];
+      double *dst = a.out + 3 * n;
+      if (MODE == H3_APPLY || MODE == H3_DIR) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double ap = ((fm >> c) & 1u) ? own[c] : o[c];
+          dst[c] = ap;
+          acc[0] = fma(own[c], ap, acc[0]);
+        }
+      } else if (MODE == H3_RES) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double ku = ((fm >> c) & 1u) ? own[c] : o[c];
+          const double r = a.f[3 * n + c] - ku;
+          dst[c] = r;
+          double z = r;
+          if (PRE == TPO_PRECOND_JACOBI) {
+            z = r / a.diag[3 * n + c];
+            a.z[3 * n + c] = z;
+          }
+          acc[0] = fma(r, z, acc[0]);
+          acc[1] = fma(r, r, acc[1]);
+        }
+      } else {  // H3_BLOCK
+        const double s = inv_sqrt_count(g, x, iy, iz);
+        const double *r = a.x + 3 * n;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double z = ((fm >> c) & 1u) ? 0.0 : o[c] * s;
+          dst[c] = z;
+          acc[0] = fma(r[c], z, acc[0]);
+          acc[1] = fma(r[c], r[c], acc[1]);
+        }
+      }
+    }
+    __syncthreads();  // the next step overwrites plane x-1 and element plane x-1
+  }
+  uint32_t *counter = MODE == H3_APPLY ? a.counter : &ctl->counter;
+  if (!grid_reduce<2>(acc, a.part, counter)) return;
+  if (threadIdx.x != 0) return;
+  if (MODE == H3_APPLY) {
+    if (a.pap_out) *a.pap_out = acc[0];
+  } else if (MODE == H3_DIR) {
+    const double pap = acc[0];
+    ctl->pap = pap;
+    ctl->first = 0;
+    if (!finite(pap)) ctl->status = TPO_SOLVE_NONFINITE;
+    else if (fabs(pap) < 1e-30) ctl->status = TPO_SOLVE_BREAKDOWN;  // solver.py:114-115
+    else ctl->alpha = ctl->rz / pap;                                  // solver.py:117
+  } else if (MODE == H3_RES || a.init) {
+    ctl->it = 0;
+    ctl->first = 1;
+    ctl->rz = acc[0];
+    ctl->rr = acc[1];
+    if (!finite(acc[0]) || !finite(acc[1])) ctl->status = TPO_SOLVE_NONFINITE;
+  } else {
+    finish_update(ctl, acc[0], acc[1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Pointwise kernels
 // ---------------------------------------------------------------------------
 // u += alpha p', r -= alpha ap; Jacobi / none: z = r / diag (or r), r.z,

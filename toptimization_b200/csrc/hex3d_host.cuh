@@ -35,6 +35,53 @@ dim3 hex_gather_grid(const Hex3 &h) { return flat_grid(h.nodes(), H3_THREADS, kH
 dim3 hex_elem_grid(const Hex3 &h) { return flat_grid(h.elems(), H3_THREADS, kHexMaxCtas); }
 dim3 hex_flat_grid(int64_t n) { return flat_grid(n, H3_FLAT, kHexMaxCtas); }
 
+// Launch plan of the nodal gathers: the plane-marching kernel when its
+// staging fits in shared memory (nelz up to ~1300) and one x-plane takes at
+// most kHexMaxCtas CTAs, the per-node kernel otherwise. About four CTAs per
+// SM: the planes are split into chunks of xc consecutive planes.
+constexpr size_t kTileSmemMax = 220 * 1024;
+struct GatherPlan {
+  bool tile = false;
+  dim3 grid;
+  int xc = 0;
+  size_t smem = 0;
+};
+
+GatherPlan gather_plan(const Hex3 &h) {
+  GatherPlan p;
+  const int64_t P = (int64_t)(h.ny + 1) * (h.nz + 1);
+  const int64_t cpp = (P + HT_THREADS - 1) / HT_THREADS;
+  const size_t smem = hex_tile_smem(h.nz);
+  if (smem > kTileSmemMax || cpp > kHexMaxCtas) {
+    p.grid = hex_gather_grid(h);
+    return p;
+  }
+  const int64_t planes = (int64_t)h.nx + 1;
+  int64_t chunks = std::max<int64_t>(1, (4 * 148 + cpp - 1) / cpp);
+  chunks = std::min<int64_t>(std::min<int64_t>(chunks, planes), kHexMaxCtas / cpp);
+  const int64_t xc = (planes + chunks - 1) / chunks;
+  chunks = (planes + xc - 1) / xc;
+  p.tile = true;
+  p.grid = dim3((unsigned)cpp, (unsigned)chunks, 1);
+  p.xc = (int)xc;
+  p.smem = smem;
+  return p;
+}
+
+template <int MODE, int PRE>
+int launch_gather(const GatherPlan &p, const Hex3Args &a, cudaStream_t st) {
+  if (p.tile) {
+    if (p.smem > 48 * 1024)
+      TPO_CK(cudaFuncSetAttribute(k_hex_tile<MODE, PRE>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
+    k_hex_tile<MODE, PRE><<<p.grid, HT_THREADS, p.smem, st>>>(a, p.xc);
+  } else {
+    k_hex_gather<MODE, PRE><<<p.grid, H3_THREADS, 0, st>>>(a);
+  }
+  TPO_CK_LAUNCH();
+  return TPO_OK;
+}
+
 struct Pcg3Ws {
   PcgCtl *ctl;
   double *s, *w, *diag, *r, *z, *pa, *pb, *ap, *part;
@@ -69,6 +116,7 @@ int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const do
   const double fn = std::sqrt(c->f_norm_sq);
   const double tol_sq = (c->tol * fn) * (c->tol * fn);
   const dim3 gg = hex_gather_grid(h), fg = hex_flat_grid(nd);
+  const GatherPlan gp = gather_plan(h);
   // warm start from u with its fixed DOFs zeroed, else from zero (solver.py:52-57)
   if (c->warm_start) {
     k_hex_zero_fixed<<<hex_flat_grid(nn), H3_FLAT, 0, st>>>(nn, fixed, u);
@@ -98,8 +146,8 @@ int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const do
   a.diag = w.diag;
   a.out = w.r;
   a.z = w.z;
-  k_hex_gather<H3_RES, PRE><<<gg, H3_THREADS, 0, st>>>(a);
-  TPO_CK_LAUNCH();
+  int rc = launch_gather<H3_RES, PRE>(gp, a, st);
+  if (rc) return rc;
   Hex3Args b{};  // element-block z = M r
   b.g = h;
   b.w = w.w;
@@ -110,8 +158,7 @@ int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const do
   b.ctl = w.ctl;
   if (PRE == TPO_PRECOND_BLOCK_JACOBI) {
     b.init = 1;
-    k_hex_gather<H3_BLOCK, 0><<<gg, H3_THREADS, 0, st>>>(b);
-    TPO_CK_LAUNCH();
+    if ((rc = launch_gather<H3_BLOCK, 0>(gp, b, st))) return rc;
     b.init = 0;
   }
   Hex3Args d{};  // p' = z + beta p, ap = K p', alpha
@@ -127,17 +174,14 @@ int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const do
 
   auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
-    k_hex_gather<H3_DIR, 0><<<gg, H3_THREADS, 0, st>>>(d);
-    TPO_CK_LAUNCH();
+    int r = launch_gather<H3_DIR, 0>(gp, d, st);
+    if (r) return r;
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
     k_hex_update<PRE><<<fg, H3_FLAT, 0, st>>>(nd, u, w.r, w.pa, w.pb, w.ap, w.diag, w.z, w.part,
                                               w.ctl);
     TPO_CK_LAUNCH();
-    if (PRE == TPO_PRECOND_BLOCK_JACOBI) {
-      k_hex_gather<H3_BLOCK, 0><<<gg, H3_THREADS, 0, st>>>(b);
-      TPO_CK_LAUNCH();
-    }
+    if (PRE == TPO_PRECOND_BLOCK_JACOBI && (r = launch_gather<H3_BLOCK, 0>(gp, b, st))) return r;
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
     return TPO_OK;
   };
@@ -149,7 +193,7 @@ int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const do
               (PRE == TPO_PRECOND_BLOCK_JACOBI ? 2 * nd * 8 + ne * 8 + nn : 0);
   PcgCtl fin;
   const int chunk = c->poll_every > 0 ? c->poll_every : 16;
-  int rc = run_iterations(iter, w.ctl, c->max_iter, 0, chunk, st, &fin, lb);
+  rc = run_iterations(iter, w.ctl, c->max_iter, 0, chunk, st, &fin, lb);
   if (rc) return rc;
   int status = fin.status;
   if (status == TPO_SOLVE_RUNNING) status = TPO_SOLVE_MAX_ITER;  // max_iter <= 0
@@ -268,8 +312,7 @@ int tpo3_matvec_f64(const tpo_grid3 *g, const double *rho, const uint8_t *fixed,
   cudaEvent_t *ev = nullptr;
   if (g_prof_on && (rc = prof_events(1, &ev))) return rc;
   if (ev) TPO_CK(cudaEventRecord(ev[0], st));
-  k_hex_gather<H3_APPLY, 0><<<hex_gather_grid(h), H3_THREADS, 0, st>>>(a);
-  TPO_CK_LAUNCH();
+  if ((rc = launch_gather<H3_APPLY, 0>(gather_plan(h), a, st))) return rc;
   if (ev) {
     TPO_CK(cudaEventRecord(ev[1], st));
     TPO_CK(cudaEventSynchronize(ev[1]));
