@@ -155,7 +155,12 @@ def test_pcg3_vs_oracle_cantilever(pre):
 def test_pcg3_per_node_kernel_path(pre):
     """A 3x2x1300 column (front face clamped, load on the back face): nelz is
     too large for the plane staging, so every gather runs the per-node kernel.
-    Exactly 200 iterations (unconverged) against the oracle's 200."""
+    Exactly 30 iterations (unconverged) against the oracle's 30. The column is
+    so ill-conditioned that rounding grows fast in its unconverged iterates:
+    two FP64 oracles that differ only in summation order (assembled vs
+    element-by-element) agree to 6e-14 / 6e-10 / 2e-12 (jacobi /
+    element-block / none) after 30 iterations but only to 3e-5 / 1e-3 / 1e-4
+    after 200, so 30 it is."""
     nx, ny, nz = 3, 2, 1300
     rng = np.random.default_rng(11)
     rho = rng.uniform(0.05, 1.0, nx * ny * nz)
@@ -164,17 +169,15 @@ def test_pcg3_per_node_kernel_path(pre):
     fixed = np.sort(np.concatenate([3 * nodes[iz == 0] + c for c in range(3)]))
     loads = [(3 * n + 1, -0.1) for n in nodes[iz == nz]]
     mesh, f, m = _system(nx, ny, nz, fixed, loads)
-    ref = O.pcg(mesh, O.simp_scale(rho, 1e-9, 3.0), f, np.zeros(mesh.n_dofs), 1e-14, 200, pre,
+    ref = O.pcg(mesh, O.simp_scale(rho, 1e-9, 3.0), f, np.zeros(mesh.n_dofs), 1e-14, 30, pre,
                 assemble=False)
     assert ref.status == "max_iter"
-    s = PCGSolver(nx, ny, 1e-9, 3.0, float(f @ f), preconditioner=pre, max_iter=200, tol=1e-14,
+    s = PCGSolver(nx, ny, 1e-9, 3.0, float(f @ f), preconditioner=pre, max_iter=30, tol=1e-14,
                   nelz=nz)
     u = torch.zeros(mesh.n_dofs, dtype=torch.float64, device=DEV)
     info = s.solve(dev(rho), dev(f), m, u, warm_start=False)
-    assert info.status == "max_iter" and info.updates == 200
-    # 200 unconverged steps amplify rounding differences; a wrong index
-    # would give O(1) differences
-    assert rel(u.cpu().numpy(), ref.u) < 1e-7
+    assert info.status == "max_iter" and info.updates == 30
+    assert rel(u.cpu().numpy(), ref.u) < 1e-8
 
 
 def test_pcg3_max_iter_and_zero_rhs():
