@@ -299,20 +299,39 @@ __global__ void __launch_bounds__(H3_THREADS) k_hex_gather(Hex3Args a) {
 // values (direction: p' = z + beta p, formed ONCE per node) are staged per
 // plane in shared memory for the run j0-(nelz+2) .. j0+T+nelz+1, which holds
 // every y/z neighbour of the CTA's nodes, in a ring of three planes (x-1, x,
-// x+1); element weights in a ring of two element planes. Global loads are
-// contiguous runs of each plane; the 27-point gather reads shared memory.
+// x+1); element weights in a ring of three element planes. The 27-point
+// gather reads shared memory.
 // Neighbours that wrap around a z-row are never used with a nonzero weight:
 // every element containing them lies outside the grid, and those weights are
-// zero. Layout of the dynamic shared memory (doubles):
+// zero.
+// Pipelining: while plane x is computed, plane x+2's node values (raw, as
+// they lie in memory: a contiguous run per plane) and element plane x+1 are
+// already on their way into shared memory by cp.async; at the next step the
+// raw run is turned into the ring's layout (p' = z + beta p, or the
+// element-block scaling). Two barriers per plane; no global load waits in the
+// compute loop. Layout of the dynamic shared memory (doubles):
 //   nodes  [3 planes][3 components][NH],  NH = T + 2*(nelz+2)
-//   elems  [2 planes][EH],                EH = T + nelz + 2
+//   raw    [2 arrays][3*NH]               (z and p for the direction)
+//   elems  [3 planes][EH],                EH = T + nelz + 2
 // ---------------------------------------------------------------------------
 constexpr int HT_THREADS = 256;
 
 __host__ __device__ inline int hex_tile_nh(int nz) { return HT_THREADS + 2 * (nz + 2); }
 __host__ __device__ inline int hex_tile_eh(int nz) { return HT_THREADS + nz + 2; }
 __host__ __device__ inline size_t hex_tile_smem(int nz) {
-  return (size_t)(9 * hex_tile_nh(nz) + 2 * hex_tile_eh(nz)) * sizeof(double);
+  return (size_t)(15 * hex_tile_nh(nz) + 3 * hex_tile_eh(nz)) * sizeof(double);
+}
+
+// 8-byte asynchronous global -> shared copy (no register staging)
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 template <int MODE, int PRE>
@@ -326,7 +345,8 @@ __global__ void __launch_bounds__(HT_THREADS) k_hex_tile(Hex3Args a, int xc) {
   const int64_t PE = (int64_t)g.ny * g.nz;      // elements per x-plane
   const int NH = hex_tile_nh(g.nz), EH = hex_tile_eh(g.nz);
   double *sv = hs;            // node ring
-  double *se = hs + 9 * NH;   // element ring
+  double *sr = hs + 9 * NH;   // raw node run(s) of the next plane
+  double *se = sr + 6 * NH;   // element ring
   const int64_t j0 = (int64_t)blockIdx.x * HT_THREADS;
   const int xa = blockIdx.y * xc, xb = min(xa + xc, g.nx + 1);
   const int64_t j = j0 + threadIdx.x;
@@ -348,61 +368,97 @@ __global__ void __launch_bounds__(HT_THREADS) k_hex_tile(Hex3Args a, int xc) {
     pnew = odd ? a.pa : a.pb;
   }
 
-  auto load_nodes = [&](int x, int slot) {
-    double *d = sv + slot * 3 * NH;
+  const int64_t jA = j0 - hoff;  // first staged plane index
+  const bool two = MODE == H3_DIR && !first;
+  // node plane x: its raw run (z and p for the direction) -> sr, by cp.async
+  auto issue_nodes = [&](int x) {
+    const bool xin = x >= 0 && x <= g.nx;
+    for (int t = threadIdx.x; t < 3 * NH; t += HT_THREADS) {
+      const int64_t jj = jA + t / 3;
+      if (xin && jj >= 0 && jj < P) {
+        const int64_t off = 3 * ((int64_t)x * P + jA) + t;
+        cp_async8(sr + t, a.x + off);
+        if (two) cp_async8(sr + 3 * NH + t, pold + off);
+      } else {
+        sr[t] = 0.0;
+        if (two) sr[3 * NH + t] = 0.0;
+      }
+    }
+  };
+  // element plane ex -> element slot (ex + 3) % 3, by cp.async
+  auto issue_elems = [&](int ex) {
+    double *d = se + ((ex + 3) % 3) * EH;
+    const bool xin = ex >= 0 && ex < g.nx;
+    for (int i = threadIdx.x; i < EH; i += HT_THREADS) {
+      const int64_t k = kmin + i;
+      if (xin && k >= 0 && k < PE) cp_async8(d + i, a.w + (int64_t)ex * PE + k);
+      else d[i] = 0.0;
+    }
+  };
+  // raw run of node plane x -> node slot (x + 3) % 3 (component-major)
+  auto combine = [&](int x) {
+    double *d = sv + ((x + 3) % 3) * 3 * NH;
     for (int i = threadIdx.x; i < NH; i += HT_THREADS) {
-      const int64_t jj = j0 - hoff + i;
-      double v[3] = {0.0, 0.0, 0.0};
-      if (x >= 0 && x <= g.nx && jj >= 0 && jj < P) {
-        const int64_t m = (int64_t)x * P + jj;
-        const double *src = a.x + 3 * m;
+      double v[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) v[c] = src[c];
-        if (MODE == H3_DIR) {
-          if (!first) {
-            const double *po = pold + 3 * m;
+      for (int c = 0; c < 3; ++c) v[c] = sr[3 * i + c];
+      const int64_t jj = jA + i;
+      if (MODE == H3_DIR) {
+        if (two) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) v[c] = fma(beta, po[c], v[c]);
-          }
-          // the CTA's own nodes: store the new direction once
-          if (x >= xa && x < xb && i >= hoff && i < hoff + HT_THREADS) {
-            double *pn = pnew + 3 * m;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) pn[c] = v[c];
-          }
+          for (int c = 0; c < 3; ++c) v[c] = fma(beta, sr[3 * NH + 3 * i + c], v[c]);
         }
-        if (MODE == H3_BLOCK) {
-          const int my = (int)(jj / nz1), mz = (int)(jj - (int64_t)my * nz1);
-          const double s = inv_sqrt_count(g, x, my, mz);
+        // the CTA's own nodes: store the new direction once
+        if (x >= xa && x < xb && i >= hoff && i < hoff + HT_THREADS && jj < P) {
+          double *pn = pnew + 3 * ((int64_t)x * P + jj);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) v[c] *= s;
+          for (int c = 0; c < 3; ++c) pn[c] = v[c];
         }
+      }
+      if (MODE == H3_BLOCK && x >= 0 && x <= g.nx && jj >= 0 && jj < P) {
+        const int my = (int)(jj / nz1), mz = (int)(jj - (int64_t)my * nz1);
+        const double sc = inv_sqrt_count(g, x, my, mz);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] *= sc;
       }
 #pragma unroll
       for (int c = 0; c < 3; ++c) d[c * NH + i] = v[c];
     }
   };
-  auto load_elems = [&](int ex, int slot) {
-    double *d = se + slot * EH;
-    for (int i = threadIdx.x; i < EH; i += HT_THREADS) {
-      const int64_t k = kmin + i;
-      d[i] = (ex >= 0 && ex < g.nx && k >= 0 && k < PE) ? a.w[(int64_t)ex * PE + k] : 0.0;
-    }
-  };
 
-  load_nodes(xa - 1, (xa + 2) % 3);
-  load_nodes(xa, xa % 3);
-  load_elems(xa - 1, (xa + 1) % 2);
+  // prologue: planes xa-1 and xa staged, plane xa+1 and element plane xa in flight
+  issue_nodes(xa - 1);
+  issue_elems(xa - 1);
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  combine(xa - 1);
+  __syncthreads();
+  issue_nodes(xa);
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  combine(xa);
+  __syncthreads();
+  issue_nodes(xa + 1);
+  issue_elems(xa);
+  cp_async_commit();
   double acc[2] = {0.0, 0.0};
   const int c0 = (int)(j - j0) + hoff;  // this node's slot in a staged plane
   for (int x = xa; x < xb; ++x) {
-    load_nodes(x + 1, (x + 1) % 3);
-    load_elems(x, x % 2);
-    __syncthreads();
+    cp_async_wait_all();
+    __syncthreads();  // raw = node plane x+1, element slot x%3 = element plane x
+    combine(x + 1);
+    __syncthreads();  // node slot (x+1)%3 complete, raw free
+    if (x + 1 < xb) {
+      issue_nodes(x + 2);
+      issue_elems(x + 1);
+      cp_async_commit();
+    }
     if (mine) {
       const double *pl[3] = {sv + ((x + 2) % 3) * 3 * NH, sv + (x % 3) * 3 * NH,
                              sv + ((x + 1) % 3) * 3 * NH};
-      const double *el[2] = {se + ((x + 1) % 2) * EH, se + (x % 2) * EH};
+      const double *el[2] = {se + ((x + 2) % 3) * EH, se + (x % 3) * EH};
       double we[8];
 #pragma unroll
       for (int ex = 0; ex < 2; ++ex)
@@ -462,8 +518,8 @@ __global__ void __launch_bounds__(HT_THREADS) k_hex_tile(Hex3Args a, int xc) {
         }
       }
     }
-    __syncthreads();  // the next step overwrites plane x-1 and element plane x-1
   }
+  cp_async_wait_all();
   uint32_t *counter = MODE == H3_APPLY ? a.counter : &ctl->counter;
   if (!grid_reduce<2>(acc, a.part, counter)) return;
   if (threadIdx.x != 0) return;

@@ -35,10 +35,29 @@ dim3 hex_gather_grid(const Hex3 &h) { return flat_grid(h.nodes(), H3_THREADS, kH
 dim3 hex_elem_grid(const Hex3 &h) { return flat_grid(h.elems(), H3_THREADS, kHexMaxCtas); }
 dim3 hex_flat_grid(int64_t n) { return flat_grid(n, H3_FLAT, kHexMaxCtas); }
 
+// CTAs of `kernel` resident per SM (1 if the query fails).
+template <typename K>
+int resident_ctas(K kernel, int threads, size_t smem) {
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess ||
+      nb < 1) {
+    cudaGetLastError();
+    return 1;
+  }
+  return nb;
+}
+
 // Launch plan of the nodal gathers: the plane-marching kernel when its
-// staging fits in shared memory (nelz up to ~1300) and one x-plane takes at
-// most kHexMaxCtas CTAs, the per-node kernel otherwise. About four CTAs per
-// SM: the planes are split into chunks of xc consecutive planes.
+// staging fits in shared memory (nelz up to ~700) and one x-plane takes at
+// most kHexMaxCtas CTAs, the per-node kernel otherwise. The planes are split
+// into chunks of xc consecutive planes so that the grid is one wave of
+// resident CTAs (longer marches amortise the two-plane prologue).
 constexpr size_t kTileSmemMax = 220 * 1024;
 struct GatherPlan {
   bool tile = false;
@@ -57,7 +76,8 @@ GatherPlan gather_plan(const Hex3 &h) {
     return p;
   }
   const int64_t planes = (int64_t)h.nx + 1;
-  int64_t chunks = std::max<int64_t>(1, (4 * 148 + cpp - 1) / cpp);
+  const int64_t wave = (int64_t)resident_ctas(k_hex_tile<H3_DIR, 0>, HT_THREADS, smem) * sm_count();
+  int64_t chunks = std::max<int64_t>(1, wave / cpp);
   chunks = std::min<int64_t>(std::min<int64_t>(chunks, planes), kHexMaxCtas / cpp);
   const int64_t xc = (planes + chunks - 1) / chunks;
   chunks = (planes + xc - 1) / xc;
@@ -115,8 +135,12 @@ int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const do
   const int64_t nn = h.nodes(), nd = 3 * nn, ne = h.elems();
   const double fn = std::sqrt(c->f_norm_sq);
   const double tol_sq = (c->tol * fn) * (c->tol * fn);
-  const dim3 gg = hex_gather_grid(h), fg = hex_flat_grid(nd);
+  const dim3 gg = hex_gather_grid(h);
   const GatherPlan gp = gather_plan(h);
+  // the update streams 8 vectors: one wave of resident CTAs, grid-stride
+  const dim3 fg = flat_grid(nd, H3_FLAT,
+                            std::min(kHexMaxCtas, resident_ctas(k_hex_update<PRE>, H3_FLAT, 0) *
+                                                      sm_count()));
   // warm start from u with its fixed DOFs zeroed, else from zero (solver.py:52-57)
   if (c->warm_start) {
     k_hex_zero_fixed<<<hex_flat_grid(nn), H3_FLAT, 0, st>>>(nn, fixed, u);
