@@ -690,8 +690,8 @@ def run_solid3d(args):
     cg_mean = float(np.mean([r.cg_iters for r in recs]))
     peak, peak_kind = measured_peak()
     nn = pr.n_nodes
-    names = {"dir": "k_hex_gather<DIR> (p = z + beta p, K p over the 27-node neighbourhood, "
-                    "p.Kp)",
+    names = {"dir": "k_hex_tile<DIR> (p = z + beta p staged plane by plane in shared memory "
+                    "by cp.async, K p over the 27-node neighbourhood, p.Kp)",
              "update": "k_hex_update<jacobi> (u, r update, z = r / diag, r.z, ||r||^2)"}
     key = max(kern, key=lambda k: kern[k]["total_ms"])
     kd = kern[key]
