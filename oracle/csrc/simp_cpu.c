@@ -1,5 +1,6 @@
 /*
- * simp_cpu.c -- C/OpenMP restatement of the reference's SIMP loop, FP64.
+ * simp_cpu.c -- C/OpenMP restatement of the reference's SIMP loop, FP64,
+ * on 2D (Q4) and 3D (H8) structured grids.
  *
  * TEST AND BASELINE INFRASTRUCTURE ONLY: used by tests/ as a fast oracle and
  * by bench.py as the timed CPU baseline (the reference's own CPU path runs on
@@ -7,16 +8,19 @@
  *
  * It follows the reference algorithm kernel by kernel, in the reference's
  * element-scatter form (tomohiron907/toptimization, src/toptimization/):
- *   matvec        fem/kernels.py:143-176   (4-colour element scatter, so the
+ *   matvec        fem/kernels.py:143-212   (element scatter in 4 (2D) or 8
+ *                                           (3D) parity colours, so the
  *                                           parallel scatter needs no atomics)
- *   jacobi diag   fem/kernels.py:76-101
- *   element block fem/preconditioner.py:19-108, fem/fields.py:133-143
+ *   jacobi diag   fem/kernels.py:76-129
+ *   element block fem/preconditioner.py:19-156, fem/fields.py:133-143
  *   PCG           fem/solver.py:27-159
- *   sensitivity   fem/kernels.py:234-272
+ *   sensitivity   fem/kernels.py:234-308
  *   filters       optimizer/filter.py:22-171 (weights recomputed per box)
  *   OC            optimizer/oc.py:21-93
  *   SIMP loop     optimizer/simp.py:141-219
- * plus the 2x2 nodal block-Jacobi option, which has no reference counterpart.
+ * plus the 2x2 nodal block-Jacobi option (2D only), which has no reference
+ * counterpart. 3D numbering (mesh.py:68-112): node (ix*(ny+1)+iy)*(nz+1)+iz,
+ * element (ex*ny+ey)*nz+ez, H8 corners bottom face then top face.
  */
 #include <math.h>
 #include <stdint.h>
@@ -30,22 +34,45 @@
 enum { PC_NONE = 0, PC_JACOBI = 1, PC_BLOCK = 2, PC_NODAL = 3 };
 
 typedef struct {
-  int nx, ny, precond, max_cg, filter_sens;
+  int nx, ny, nz, dim, dpe, precond, max_cg, filter_sens; /* nz = 0: 2D */
   double e_min, pen, rmin, volfrac, move, cg_tol, alpha_reg, f_norm;
   size_t nn, ndof, ne;
-  double ke[64], kinv[64];
+  double *ke, *kinv; /* dpe x dpe */
   double *f, *u, *r, *p, *ap, *z, *diag, *scale, *w;
   double *rho, *rho_phys, *dc, *dc_filt, *tmp, *binv; /* binv: 3 per node */
   uint8_t *fixed; /* per DOF */
   int it;
 } ocpu;
 
-static inline void elem_dofs(const ocpu *c, int ex, int ey, long d[8]) {
+/* DOFs of element (ex, ey, ez) in the reference's order (ez = 0 in 2D) */
+static inline void elem_dofs(const ocpu *c, int ex, int ey, int ez, long d[24]) {
   const long ny1 = c->ny + 1;
-  const long n1 = ex * ny1 + ey, n2 = (ex + 1) * ny1 + ey, n3 = n2 + 1, n4 = n1 + 1;
-  d[0] = 2 * n1; d[1] = 2 * n1 + 1; d[2] = 2 * n2; d[3] = 2 * n2 + 1;
-  d[4] = 2 * n3; d[5] = 2 * n3 + 1; d[6] = 2 * n4; d[7] = 2 * n4 + 1;
+  if (c->dim == 2) {
+    const long n1 = ex * ny1 + ey, n2 = (ex + 1) * ny1 + ey, n3 = n2 + 1, n4 = n1 + 1;
+    d[0] = 2 * n1; d[1] = 2 * n1 + 1; d[2] = 2 * n2; d[3] = 2 * n2 + 1;
+    d[4] = 2 * n3; d[5] = 2 * n3 + 1; d[6] = 2 * n4; d[7] = 2 * n4 + 1;
+    return;
+  }
+  static const int cx[8] = {0, 1, 1, 0, 0, 1, 1, 0}, cy[8] = {0, 0, 1, 1, 0, 0, 1, 1},
+                   cz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+  const long nz1 = c->nz + 1;
+  for (int k = 0; k < 8; ++k) {
+    const long n = ((long)(ex + cx[k]) * ny1 + ey + cy[k]) * nz1 + ez + cz[k];
+    d[3 * k] = 3 * n; d[3 * k + 1] = 3 * n + 1; d[3 * k + 2] = 3 * n + 2;
+  }
 }
+
+static inline long elem_index(const ocpu *c, int ex, int ey, int ez) {
+  return c->dim == 2 ? (long)ex * c->ny + ey : ((long)ex * c->ny + ey) * c->nz + ez;
+}
+static inline void elem_coords(const ocpu *c, long e, int *ex, int *ey, int *ez) {
+  if (c->dim == 2) {
+    *ex = (int)(e / c->ny); *ey = (int)(e % c->ny); *ez = 0;
+  } else {
+    *ez = (int)(e % c->nz); *ey = (int)((e / c->nz) % c->ny); *ex = (int)(e / ((long)c->nz * c->ny));
+  }
+}
+static inline int ncolors(const ocpu *c) { return c->dim == 2 ? 4 : 8; }
 
 static double dot(const double *a, const double *b, size_t n) {
   double s = 0.0;
@@ -54,24 +81,28 @@ static double dot(const double *a, const double *b, size_t n) {
   return s;
 }
 
-/* out = sum_e s_e M p_e (element scatter, 4 colours), M = Ke or Ke_inv. */
+/* out = sum_e s_e M p_e (element scatter in parity colours: elements of one
+ * colour share no node), M = Ke or Ke_inv. */
 static void scatter_apply(const ocpu *c, const double *m, const double *s, const double *in,
                           double *out) {
   memset(out, 0, c->ndof * sizeof(double));
-  for (int color = 0; color < 4; ++color) {
-    const int cx = color & 1, cy = color >> 1;
+  const int dpe = c->dpe, nzl = c->dim == 2 ? 1 : c->nz;
+  for (int color = 0; color < ncolors(c); ++color) {
+    const int cx = color & 1, cy = (color >> 1) & 1, cz = color >> 2;
 #pragma omp parallel for schedule(static)
     for (int ex = cx; ex < c->nx; ex += 2) {
       for (int ey = cy; ey < c->ny; ey += 2) {
-        long d[8];
-        elem_dofs(c, ex, ey, d);
-        const double se = s[(long)ex * c->ny + ey];
-        double pl[8];
-        for (int j = 0; j < 8; ++j) pl[j] = in[d[j]];
-        for (int i = 0; i < 8; ++i) {
-          double acc = 0.0;
-          for (int j = 0; j < 8; ++j) acc += m[i * 8 + j] * pl[j];
-          out[d[i]] += se * acc;
+        for (int ez = cz; ez < nzl; ez += 2) {
+          long d[24];
+          elem_dofs(c, ex, ey, ez, d);
+          const double se = s[elem_index(c, ex, ey, ez)];
+          double pl[24];
+          for (int j = 0; j < dpe; ++j) pl[j] = in[d[j]];
+          for (int i = 0; i < dpe; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < dpe; ++j) acc += m[i * dpe + j] * pl[j];
+            out[d[i]] += se * acc;
+          }
         }
       }
     }
@@ -87,17 +118,19 @@ static void matvec(const ocpu *c, const double *p, double *ap) {
 
 static void setup_precond(ocpu *c) {
   if (c->precond == PC_JACOBI) {
+    const int dpe = c->dpe, nzl = c->dim == 2 ? 1 : c->nz;
     memset(c->diag, 0, c->ndof * sizeof(double));
-    for (int color = 0; color < 4; ++color) {
-      const int cx = color & 1, cy = color >> 1;
+    for (int color = 0; color < ncolors(c); ++color) {
+      const int cx = color & 1, cy = (color >> 1) & 1, cz = color >> 2;
 #pragma omp parallel for schedule(static)
       for (int ex = cx; ex < c->nx; ex += 2)
-        for (int ey = cy; ey < c->ny; ey += 2) {
-          long d[8];
-          elem_dofs(c, ex, ey, d);
-          const double se = c->scale[(long)ex * c->ny + ey];
-          for (int i = 0; i < 8; ++i) c->diag[d[i]] += se * c->ke[i * 9];
-        }
+        for (int ey = cy; ey < c->ny; ey += 2)
+          for (int ez = cz; ez < nzl; ez += 2) {
+            long d[24];
+            elem_dofs(c, ex, ey, ez, d);
+            const double se = c->scale[elem_index(c, ex, ey, ez)];
+            for (int i = 0; i < dpe; ++i) c->diag[d[i]] += se * c->ke[i * (dpe + 1)];
+          }
     }
 #pragma omp parallel for schedule(static)
     for (long i = 0; i < (long)c->ndof; ++i) {
@@ -110,12 +143,19 @@ static void setup_precond(ocpu *c) {
       const double s = c->scale[e], sc = s > c->alpha_reg ? s : c->alpha_reg;
       c->w[e] = s / (sc * sc);
     }
-    /* diag holds 1/sqrt(count) per DOF */
+    /* diag holds 1/sqrt(count) per DOF: elements sharing the node */
 #pragma omp parallel for schedule(static)
     for (long n = 0; n < (long)c->nn; ++n) {
-      const int x = (int)(n / (c->ny + 1)), y = (int)(n % (c->ny + 1));
-      const int cnt = ((x >= 1) + (x <= c->nx - 1)) * ((y >= 1) + (y <= c->ny - 1));
-      c->diag[2 * n] = c->diag[2 * n + 1] = 1.0 / sqrt((double)cnt);
+      int x, y, z = 0;
+      if (c->dim == 2) {
+        x = (int)(n / (c->ny + 1)); y = (int)(n % (c->ny + 1));
+      } else {
+        z = (int)(n % (c->nz + 1)); y = (int)((n / (c->nz + 1)) % (c->ny + 1));
+        x = (int)(n / ((long)(c->nz + 1) * (c->ny + 1)));
+      }
+      int cnt = ((x >= 1) + (x <= c->nx - 1)) * ((y >= 1) + (y <= c->ny - 1));
+      if (c->dim == 3) cnt *= (z >= 1) + (z <= c->nz - 1);
+      for (int k = 0; k < c->dim; ++k) c->diag[c->dim * n + k] = 1.0 / sqrt((double)cnt);
     }
   } else if (c->precond == PC_NODAL) {
     double *b = c->tmp; /* 3 per node, nn <= ne + ... : use binv as scratch */
@@ -126,8 +166,8 @@ static void setup_precond(ocpu *c) {
 #pragma omp parallel for schedule(static)
       for (int ex = cx; ex < c->nx; ex += 2)
         for (int ey = cy; ey < c->ny; ey += 2) {
-          long d[8];
-          elem_dofs(c, ex, ey, d);
+          long d[24];
+          elem_dofs(c, ex, ey, 0, d);
           const double se = c->scale[(long)ex * c->ny + ey];
           for (int a = 0; a < 4; ++a) {
             const long n = d[2 * a] / 2;
@@ -218,20 +258,25 @@ static int pcg(ocpu *c, int warm, int *status_out) {
 /* hat filter over the in-domain box, reference neighbour order */
 static void hat_filter(const ocpu *c, const double *x, const double *rho, double *out, int sens) {
   const int R = (int)ceil(c->rmin);
+  const int Rz = c->dim == 2 ? 0 : R, nzl = c->dim == 2 ? 1 : c->nz;
 #pragma omp parallel for schedule(static)
   for (long e = 0; e < (long)c->ne; ++e) {
-    const int ex = (int)(e / c->ny), ey = (int)(e % c->ny);
+    int ex, ey, ez;
+    elem_coords(c, e, &ex, &ey, &ez);
     double num = 0.0, den = 0.0;
     for (int jx = ex - R; jx <= ex + R; ++jx) {
       if (jx < 0 || jx >= c->nx) continue;
       for (int jy = ey - R; jy <= ey + R; ++jy) {
         if (jy < 0 || jy >= c->ny) continue;
-        const double dx = ex - jx, dy = ey - jy;
-        const double w = c->rmin - sqrt(dx * dx + dy * dy);
-        if (w > 0.0) {
-          const long j = (long)jx * c->ny + jy;
-          num += sens ? w * rho[j] * x[j] : w * x[j];
-          den += w;
+        for (int jz = ez - Rz; jz <= ez + Rz; ++jz) {
+          if (jz < 0 || jz >= nzl) continue;
+          const double dx = ex - jx, dy = ey - jy, dz = ez - jz;
+          const double w = c->rmin - sqrt(dx * dx + dy * dy + dz * dz);
+          if (w > 0.0) {
+            const long j = elem_index(c, jx, jy, jz);
+            num += sens ? w * rho[j] * x[j] : w * x[j];
+            den += w;
+          }
         }
       }
     }
@@ -243,13 +288,16 @@ static double sensitivity(const ocpu *c, const double *rho) {
   double comp = 0.0;
 #pragma omp parallel for reduction(+ : comp) schedule(static)
   for (long e = 0; e < (long)c->ne; ++e) {
-    long d[8];
-    elem_dofs(c, (int)(e / c->ny), (int)(e % c->ny), d);
-    double ul[8], uku = 0.0;
-    for (int j = 0; j < 8; ++j) ul[j] = c->u[d[j]];
-    for (int i = 0; i < 8; ++i) {
+    int ex, ey, ez;
+    elem_coords(c, e, &ex, &ey, &ez);
+    long d[24];
+    elem_dofs(c, ex, ey, ez, d);
+    const int dpe = c->dpe;
+    double ul[24], uku = 0.0;
+    for (int j = 0; j < dpe; ++j) ul[j] = c->u[d[j]];
+    for (int i = 0; i < dpe; ++i) {
       double ku = 0.0;
-      for (int j = 0; j < 8; ++j) ku += c->ke[i * 8 + j] * ul[j];
+      for (int j = 0; j < dpe; ++j) ku += c->ke[i * dpe + j] * ul[j];
       uku += ul[i] * ku;
     }
     const double r = rho[e];
@@ -289,20 +337,28 @@ static double oc_update(ocpu *c, double *vol_out) {
 }
 
 /* ------------------------------------------------------------------ API */
-void *ocpu_create(int nx, int ny, const double ke[64], const double kinv[64], double alpha_reg,
-                  const int64_t *fixed_dofs, long n_fixed, const double *f, double e_min,
-                  double pen, double rmin, double volfrac, double move, int precond,
-                  double cg_tol, int max_cg, int filter_sens) {
+/* nz = 0: 2D (ke, kinv 8x8); nz >= 1: 3D (ke, kinv 24x24). The nodal block
+ * preconditioner is 2D only (NULL for 3D). */
+void *ocpu_create(int nx, int ny, int nz, const double *ke, const double *kinv,
+                  double alpha_reg, const int64_t *fixed_dofs, long n_fixed, const double *f,
+                  double e_min, double pen, double rmin, double volfrac, double move,
+                  int precond, double cg_tol, int max_cg, int filter_sens) {
+  if (nz > 0 && precond == PC_NODAL) return NULL;
   ocpu *c = (ocpu *)calloc(1, sizeof(ocpu));
   if (!c) return NULL;
-  c->nx = nx; c->ny = ny; c->precond = precond; c->max_cg = max_cg;
+  c->nx = nx; c->ny = ny; c->nz = nz > 0 ? nz : 0; c->dim = nz > 0 ? 3 : 2;
+  c->dpe = c->dim == 2 ? 8 : 24;
+  c->precond = precond; c->max_cg = max_cg;
   c->filter_sens = filter_sens; c->e_min = e_min; c->pen = pen; c->rmin = rmin;
   c->volfrac = volfrac; c->move = move; c->cg_tol = cg_tol; c->alpha_reg = alpha_reg;
-  c->nn = (size_t)(nx + 1) * (ny + 1);
-  c->ndof = 2 * c->nn;
-  c->ne = (size_t)nx * ny;
-  memcpy(c->ke, ke, sizeof(c->ke));
-  memcpy(c->kinv, kinv, sizeof(c->kinv));
+  c->nn = (size_t)(nx + 1) * (ny + 1) * (c->dim == 3 ? (size_t)(nz + 1) : 1);
+  c->ndof = (size_t)c->dim * c->nn;
+  c->ne = (size_t)nx * ny * (c->dim == 3 ? (size_t)nz : 1);
+  const size_t km = (size_t)c->dpe * c->dpe;
+  c->ke = (double *)malloc(km * sizeof(double));
+  c->kinv = (double *)malloc(km * sizeof(double));
+  memcpy(c->ke, ke, km * sizeof(double));
+  memcpy(c->kinv, kinv, km * sizeof(double));
   const size_t nd = c->ndof, ne = c->ne;
   double **vecs[] = {&c->f, &c->u, &c->r, &c->p, &c->ap, &c->z, &c->diag};
   for (size_t i = 0; i < sizeof(vecs) / sizeof(vecs[0]); ++i)
@@ -329,6 +385,8 @@ void ocpu_destroy(void *h) {
                    c->rho_phys, c->dc, c->dc_filt, c->tmp, c->binv};
   for (size_t i = 0; i < sizeof(all) / sizeof(all[0]); ++i) free(all[i]);
   free(c->fixed);
+  free(c->ke);
+  free(c->kinv);
   free(c);
 }
 

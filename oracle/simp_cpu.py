@@ -12,7 +12,7 @@ from ctypes import POINTER, c_double, c_int, c_long, c_void_p
 import numpy as np
 
 from . import build_c
-from toptimization_b200.material import compute_Ke_2d, regularized_inverse
+from toptimization_b200.material import compute_Ke, regularized_inverse
 from toptimization_b200.mesh import force_vector
 
 PRECOND = {"none": 0, "jacobi": 1, "block_jacobi": 2, "nodal_block_jacobi": 3}
@@ -25,7 +25,8 @@ def lib():
         L = ctypes.CDLL(str(build_c.build()))
         PD = POINTER(c_double)
         L.ocpu_create.restype = c_void_p
-        L.ocpu_create.argtypes = [c_int, c_int, PD, PD, c_double, POINTER(ctypes.c_int64), c_long,
+        L.ocpu_create.argtypes = [c_int, c_int, c_int, PD, PD, c_double,
+                                  POINTER(ctypes.c_int64), c_long,
                                   PD, c_double, c_double, c_double, c_double, c_double, c_int,
                                   c_double, c_int, c_int]
         L.ocpu_destroy.argtypes = [c_void_p]
@@ -44,24 +45,26 @@ def _pd(a):
 
 
 class CpuSimp:
-    """One design on the CPU; `iteration()` runs one OC iteration."""
+    """One design on the CPU (2D or 3D); `iteration()` runs one OC iteration."""
 
     def __init__(self, problem, preconditioner=None):
         pr = problem
         self.problem = pr
-        Ke = np.ascontiguousarray(compute_Ke_2d(pr.E, pr.nu))
+        nz = pr.nelz if pr.dim == 3 else 0
+        Ke = np.ascontiguousarray(compute_Ke(pr.E, pr.nu, pr.dim))
         Kinv, alpha = regularized_inverse(Ke)
         Kinv = np.ascontiguousarray(Kinv)
         fixed = np.ascontiguousarray(np.asarray(pr.fixed_dofs, dtype=np.int64))
         f = np.ascontiguousarray(force_vector(pr))
         pre = PRECOND[preconditioner or pr.preconditioner]
-        self.h = lib().ocpu_create(pr.nelx, pr.nely, _pd(Ke), _pd(Kinv), alpha,
+        self.h = lib().ocpu_create(pr.nelx, pr.nely, nz, _pd(Ke), _pd(Kinv), alpha,
                                    fixed.ctypes.data_as(POINTER(ctypes.c_int64)), fixed.size,
                                    _pd(f), pr.E_min, pr.penalty, pr.rmin, pr.volfrac,
                                    pr.move_limit, pre, pr.cg_tol, pr.max_cg_iter,
                                    1 if pr.filter_type == "sensitivity" else 0)
         if not self.h:
-            raise MemoryError("ocpu_create failed")
+            raise ValueError("ocpu_create failed (out of memory, or the nodal block "
+                             "preconditioner on a 3D grid)")
 
     def iteration(self, max_cg: int = 0) -> dict:
         out = np.zeros(7)

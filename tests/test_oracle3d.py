@@ -143,3 +143,36 @@ def test_matrix_free_operator_matches_assembly(shape):
     a = O.pcg(m, s, p * ~m.is_fixed, np.zeros(m.n_dofs), 1e-10, 500, "jacobi")
     b = O.pcg(m, s, p * ~m.is_fixed, np.zeros(m.n_dofs), 1e-10, 500, "jacobi", assemble=False)
     assert a.iters == b.iters and rel(b.u, a.u) < 1e-12
+
+
+@pytest.mark.parametrize("name,ov,comp_tol,cg_rel", [
+    ("3d_jacobi", {}, 1e-9, 0.0),
+    ("3d_block_jacobi", dict(max_iter=8, preconditioner="block_jacobi"), 1e-8, 0.03),
+    ("3d_sensitivity", dict(max_iter=8, filter_type="sensitivity", preconditioner="none"),
+     1e-9, 0.01),
+])
+def test_c_oracle_3d_matches_reference(name, ov, comp_tol, cg_rel):
+    """The C/OpenMP restatement (the timed CPU baseline of the 3D bench) on the
+    same runs. Measured: compliance 1.3e-10 / 6.7e-10 / 1.5e-10, density
+    8.6e-10 / 2.1e-9 / 1.3e-9, CG counts +-1 / 9 / 3."""
+    from oracle import simp_cpu
+    g = golden(f"ref_run_{name}")
+    pr = load_problem(YAML / "cantilever_3d_small.yaml")
+    for k, v in ov.items():
+        setattr(pr, k, v)
+    cpu = simp_cpu.CpuSimp(pr)
+    out = [cpu.iteration() for _ in range(len(g["compliance"]))]
+    c = np.array([o["compliance"] for o in out])
+    assert np.max(np.abs(c - g["compliance"]) / g["compliance"]) < comp_tol
+    assert np.abs(cpu.rho() - g["rho_final"]).max() < 5e-8
+    cg_ref = np.asarray(g["cg_iters"])
+    cg = np.array([o["cg_iters"] for o in out])
+    assert np.all(np.abs(cg - cg_ref) <= np.maximum(1, cg_rel * cg_ref))
+    cpu.close()
+
+
+def test_c_oracle_rejects_nodal_block_in_3d():
+    from oracle import simp_cpu
+    pr = load_problem(YAML / "cantilever_3d_small.yaml")
+    with pytest.raises(ValueError):
+        simp_cpu.CpuSimp(pr, preconditioner="nodal_block_jacobi")
