@@ -147,14 +147,17 @@ def test_matrix_free_operator_matches_assembly(shape):
 
 @pytest.mark.parametrize("name,ov,comp_tol,cg_rel", [
     ("3d_jacobi", {}, 1e-9, 0.0),
-    ("3d_block_jacobi", dict(max_iter=8, preconditioner="block_jacobi"), 1e-8, 0.03),
+    ("3d_block_jacobi", dict(max_iter=8, preconditioner="block_jacobi"), 1e-8, 0.05),
     ("3d_sensitivity", dict(max_iter=8, filter_type="sensitivity", preconditioner="none"),
-     1e-9, 0.01),
+     1e-9, 0.02),
 ])
 def test_c_oracle_3d_matches_reference(name, ov, comp_tol, cg_rel):
     """The C/OpenMP restatement (the timed CPU baseline of the 3D bench) on the
     same runs. Measured: compliance 1.3e-10 / 6.7e-10 / 1.5e-10, density
-    8.6e-10 / 2.1e-9 / 1.3e-9, CG counts +-1 / 9 / 3."""
+    8.6e-10 / 2.1e-9 / 1.3e-9, CG counts +-1 / 9 / 3 (the OpenMP reduction
+    order follows the thread count, so the slow unpreconditioned and
+    element-block solves stop some iterations apart from run to run: up to 3
+    of 293 and 23 of 661 seen with 1 to 8 threads)."""
     from oracle import simp_cpu
     g = golden(f"ref_run_{name}")
     pr = load_problem(YAML / "cantilever_3d_small.yaml")
