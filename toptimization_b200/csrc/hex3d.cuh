@@ -335,7 +335,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 template <int MODE, int PRE>
-__global__ void __launch_bounds__(HT_THREADS) k_hex_tile(Hex3Args a, int xc) {
+__global__ void __launch_bounds__(HT_THREADS, 3) k_hex_tile(Hex3Args a, int xc) {
   PcgCtl *ctl = a.ctl;
   if (MODE != H3_APPLY && ctl->status != TPO_SOLVE_RUNNING) return;
   extern __shared__ double hs[];
