@@ -217,3 +217,43 @@ def test_point_location_clamped_and_region():
     p = problem_from_dict(raw)
     assert list(p.force_dofs) == [2 * (4 * 3 + 2) + 1]
     assert list(p.fixed_dofs) == sorted(2 * n + 1 for n in (3, 4, 6, 7))
+
+
+@pytest.mark.parametrize("bad, msg", [
+    ({"loads": [{"nodes": {"type": "edge", "edge": "left"}, "force": [0.0, 1.0, 0.0]}]},
+     "Unknown node spec type 'edge' for dim=3"),
+    ({"loads": [{"nodes": {"type": "face", "face": "middle"}, "force": [0.0, 1.0, 0.0]}]},
+     "Unknown face"),
+    ({"loads": [{"nodes": {"type": "point", "corner": "top-right"}, "force": [0.0, 1.0, 0.0]}]},
+     "Unknown 3D corner"),
+    ({"loads": [{"nodes": {"type": "face", "face": "top"}, "force": [0.0, 1.0]}]},
+     "force vector length 2 != dim 3"),
+    ({"boundary_conditions": {"fixed": [{"nodes": {"type": "face", "face": "left"},
+                                         "dofs": ["w"]}]}}, "Unknown DOF label"),
+])
+def test_validation_errors_3d(bad, msg):
+    """The reference's 3D parser rules (problem.py:231-263,281-367): faces only
+    in 3D, edges only in 2D, the four named 3D corners, force length = dim."""
+    raw = {"problem": {"dimension": 3}, "domain": {"nelx": 4, "nely": 2, "nelz": 3},
+           "loads": [{"nodes": {"type": "point", "corner": "back-bottom-right"},
+                      "force": [0, -1, 0]}]}
+    raw.update(bad)
+    with pytest.raises(ValueError, match=msg):
+        problem_from_dict(raw)
+
+
+def test_face_in_2d_rejected_and_3d_defaults():
+    raw = {"domain": {"nelx": 4, "nely": 2},
+           "loads": [{"nodes": {"type": "face", "face": "top"}, "force": [0, -1]}]}
+    with pytest.raises(ValueError, match="Unknown node spec type 'face' for dim=2"):
+        problem_from_dict(raw)
+    # 3D: nelz defaults to 1, fixed DOFs default to x and y only, the 3D
+    # location is not clamped, z ranges default to the whole depth
+    raw = {"problem": {"dimension": 3}, "domain": {"nelx": 2, "nely": 1},
+           "boundary_conditions": {"fixed": [{"nodes": {"type": "region", "x": [0, 0],
+                                                        "y": [0, 0]}}]},
+           "loads": [{"nodes": {"type": "point", "location": [2, 1, 1]}, "force": [0, 0, 1]}]}
+    p = problem_from_dict(raw)
+    assert p.nelz == 1 and p.n_nodes == 3 * 2 * 2 and p.n_dofs == 36
+    assert list(p.fixed_dofs) == [0, 1, 3, 4]          # nodes (0,0,0), (0,0,1): x, y
+    assert list(p.force_dofs) == [3 * ((2 * 2 + 1) * 2 + 1) + 2]
