@@ -13,7 +13,9 @@ What is recorded, all from the reference's own code:
                       filters, the OC update, a PCG solve per preconditioner)
                       on a seeded 12x5 cantilever.
   ref_kernels3d.npz   the same single calls through the reference's 3D (H8)
-                      kernels on a seeded 5x3x2 cantilever.
+                      kernels on a seeded 5x3x2 cantilever;
+  ref_kernels3d_rollers.npz  and on a 3x5x4 block on rollers (partial DOF
+                      sets on three faces) with three point loads.
   ref_run_*.npz       whole `simp.run` optimisations: compliance, volume,
                       change and CG-count histories plus final densities
                       (ref_run_3d_*: the 3D loop on an 8x4x3 cantilever).
@@ -127,6 +129,36 @@ def _small_problem_3d(nelx=5, nely=3, nelz=2):
                    output_format="png")
 
 
+def _small_problem_3d_rollers(nelx=3, nely=5, nelz=4):
+    """Rollers: y fixed on the bottom face, x on the left face, z on the front
+    face (partial DOF sets); three point loads of mixed direction."""
+    from toptimization.problem import Problem
+    ny1, nz1 = nely + 1, nelz + 1
+
+    def node(ix, iy, iz):
+        return (ix * ny1 + iy) * nz1 + iz
+    fixed = set()
+    for ix in range(nelx + 1):
+        for iz in range(nz1):
+            fixed.add(3 * node(ix, 0, iz) + 1)
+    for iy in range(ny1):
+        for iz in range(nz1):
+            fixed.add(3 * node(0, iy, iz))
+    for ix in range(nelx + 1):
+        for iy in range(ny1):
+            fixed.add(3 * node(ix, iy, 0) + 2)
+    loads = [(3 * node(nelx, nely, nelz) + 1, -1.0), (3 * node(nelx, 2, 3), 0.5),
+             (3 * node(1, nely, 2) + 2, -0.25)]
+    return Problem(name="k3b", dim=3, nelx=nelx, nely=nely, nelz=nelz, E=1.0, nu=0.3,
+                   E_min=1e-9, fixed_dofs=np.array(sorted(fixed)),
+                   force_dofs=np.array([d for d, _ in loads]),
+                   force_values=np.array([v for _, v in loads]), volfrac=0.4,
+                   penalty=3.0, rmin=1.5, filter_type="density", max_iter=1, tol=0.0,
+                   move_limit=0.2, max_cg_iter=500, cg_tol=1e-10, preconditioner="jacobi",
+                   output_dir=Path(tempfile.mkdtemp()), save_interval=10 ** 6,
+                   output_format="png")
+
+
 def _kernels(ref_src: str) -> dict:
     _import_reference(ref_src)
     pr, _ = _small_problem()
@@ -136,6 +168,11 @@ def _kernels(ref_src: str) -> dict:
 def _kernels3d(ref_src: str) -> dict:
     _import_reference(ref_src)
     return _kernel_suite(ref_src, _small_problem_3d(), 3, 20261204, (1.5, 2.2))
+
+
+def _kernels3d_rollers(ref_src: str) -> dict:
+    _import_reference(ref_src)
+    return _kernel_suite(ref_src, _small_problem_3d_rollers(), 3, 20261205, (1.2, 2.9))
 
 
 def _kernel_suite(ref_src: str, pr, dim: int, seed: int, rmin_list) -> dict:
@@ -316,6 +353,9 @@ def main():
             jobs.append(("ref_kernels", pool.apply_async(_kernels, (ref_src,))))
         if not a.only or a.only == "ref_kernels3d":
             jobs.append(("ref_kernels3d", pool.apply_async(_kernels3d, (ref_src,))))
+        if not a.only or a.only == "ref_kernels3d_rollers":
+            jobs.append(("ref_kernels3d_rollers",
+                         pool.apply_async(_kernels3d_rollers, (ref_src,))))
         for name, (y, ov, snaps) in runs.items():
             if not a.only or a.only == name:
                 jobs.append((name, pool.apply_async(_run, ((ref_src, y, ov, snaps),))))

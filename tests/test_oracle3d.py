@@ -18,16 +18,24 @@ from toptimization_b200.material import compute_Ke_3d
 from toptimization_b200.problem import load_problem
 
 KE3 = compute_Ke_3d(1.0, 0.3)
-G = golden("ref_kernels3d")
 B = golden("boundary")
 YAML = REPO / "tests" / "golden" / "yaml"
+# single-kernel fixtures: a clamped 5x3x2 cantilever, a 3x5x4 block on
+# rollers (partial DOF sets on three faces, three point loads)
+FIXTURES = {"cantilever": golden("ref_kernels3d"), "rollers": golden("ref_kernels3d_rollers")}
+RMINS = {"cantilever": (1.5, 2.2), "rollers": (1.2, 2.9)}
+
+
+@pytest.fixture(params=sorted(FIXTURES))
+def G(request):
+    return FIXTURES[request.param]
 
 
 def rel(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
-def _mesh():
+def _mesh(G):
     return O.Mesh3D(int(G["nelx"]), int(G["nely"]), int(G["nelz"]), KE3, G["fixed"])
 
 
@@ -50,8 +58,8 @@ def test_fixed_mask_3d():
     np.testing.assert_array_equal(dofs, pr.fixed_dofs)
 
 
-def test_matvec_and_diag_3d():
-    m = _mesh()
+def test_matvec_and_diag_3d(G):
+    m = _mesh(G)
     s = O.simp_scale(G["rho"], 1e-9, 3.0)
     Ap = O.assemble_K(m, s) @ G["p"]
     assert rel(Ap, G["Ap"]) < 1e-15
@@ -60,22 +68,24 @@ def test_matvec_and_diag_3d():
     np.testing.assert_array_equal(O.diag_count(m), G["diag_count"])
 
 
-def test_element_block_preconditioner_3d():
-    m = _mesh()
+def test_element_block_preconditioner_3d(G):
+    m = _mesh(G)
     z = O.block_jacobi_matrix(m, O.simp_scale(G["rho"], 1e-9, 3.0)) @ G["p2"]
     assert rel(z, G["bj_z"]) < 1e-14
     assert float(G["p2"] @ z) == pytest.approx(float(G["bj_rz"]), rel=1e-13)
     assert float(G["p2"] @ G["p2"]) == pytest.approx(float(G["bj_rr"]), rel=1e-14)
 
 
-def test_sensitivity_3d():
-    dc, c = O.sensitivity(_mesh(), G["p"], G["rho"], 1e-9, 3.0)
+def test_sensitivity_3d(G):
+    dc, c = O.sensitivity(_mesh(G), G["p"], G["rho"], 1e-9, 3.0)
     assert rel(dc, G["sens_dc"]) < 1e-14
     assert c == pytest.approx(float(G["sens_c"]), rel=1e-14)
 
 
-@pytest.mark.parametrize("rmin", [1.5, 2.2])
-def test_filters_3d(rmin):
+@pytest.mark.parametrize("name", sorted(FIXTURES))
+@pytest.mark.parametrize("k", [0, 1])
+def test_filters_3d(name, k):
+    G, rmin = FIXTURES[name], RMINS[name][k]
     H, Hs = O.filter_matrix(int(G["nelx"]), int(G["nely"]), rmin, int(G["nelz"]))
     np.testing.assert_array_equal(O.density_filter(H, Hs, G["rho"]), G[f"filt_rho_r{rmin}"])
     np.testing.assert_array_equal(O.density_filter(H, Hs, G["dc_in"]), G[f"filt_dc_r{rmin}"])
@@ -83,15 +93,15 @@ def test_filters_3d(rmin):
 
 
 @pytest.mark.parametrize("vf", [0.2, 0.4, 0.7])
-def test_oc_3d(vf):
+def test_oc_3d(G, vf):
     new, ch = O.oc_update(G["rho"], G["dc_in"], vf, 0.2)
     np.testing.assert_array_equal(new, G[f"oc_rho_vf{vf}"])
     assert ch == float(G[f"oc_change_vf{vf}"])
 
 
 @pytest.mark.parametrize("pre", ["jacobi", "block_jacobi", "none"])
-def test_pcg_3d(pre):
-    m = _mesh()
+def test_pcg_3d(G, pre):
+    m = _mesh(G)
     f = np.zeros(m.n_dofs)
     f[G["force_dofs"]] = G["force_values"]
     res = O.pcg(m, O.simp_scale(G["rho"], 1e-9, 3.0), f, np.zeros(m.n_dofs), 1e-10, 500, pre)
