@@ -169,6 +169,10 @@ int sm_count() {
 // Stencil launch configuration per kernel instantiation: dynamic shared
 // memory (set once), resident CTAs per SM, and the strip length that makes
 // the grid close to one full wave.
+#ifndef TPO_MIN_STRIP
+#define TPO_MIN_STRIP 16
+#endif
+constexpr int kMinStrip = TPO_MIN_STRIP;  // shortest stencil strip (node columns)
 template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
   static constexpr int G = 2;
   static constexpr int NG = 4;
@@ -194,7 +198,9 @@ template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
     const int rows = (ny + 1 + RPC - 1) / RPC;
     const int target = sm_count() * resident();
     int strips = std::max(1, target / rows);
-    int L = std::max(8, (nx + 1 + strips - 1) / strips);
+    // a strip recomputes two columns besides its own: keep it long enough
+    // that the overlap stays small, even if the grid is then under one wave
+    int L = std::max(kMinStrip, (nx + 1 + strips - 1) / strips);
     strips = (nx + 1 + L - 1) / L;
     return Plan{dim3(rows, strips, 1), L};
   }
@@ -245,11 +251,24 @@ template <typename T, typename C, int PRE> struct CgCfg {
   }
 };
 
-// flat update: about eight resident 256-thread CTAs per SM, grid-stride beyond
+// flat update: runs of UQ rows, one per thread, at most eight 256-thread CTAs
+// per SM (this bound sizes the partial-sum buffers); grid-stride beyond
 int update_flat_ctas(int nx, int ny) {
-  const int64_t total = (int64_t)(nx + 1) * (ny + 1);
+  const int64_t total = (int64_t)(nx + 1) * ((ny + 1 + UQ - 1) / UQ);
   const int64_t want = (total + UF_THREADS - 1) / UF_THREADS;
   return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count() * 8));
+}
+// the launched grid: one wave of the kernel's resident CTAs, within that bound
+template <auto KERN> int flat_wave(int nx, int ny) {
+  static int occ = -1;
+  if (occ < 0) {
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, KERN, UF_THREADS, 0) != cudaSuccess ||
+        o < 1)
+      o = 1;
+    occ = o;
+  }
+  return std::min(update_flat_ctas(nx, ny), sm_count() * occ);
 }
 constexpr int kBlkL = 16;
 dim3 blk_grid(int nx, int ny) {
@@ -585,7 +604,8 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
     k_blockpre<double, double, true, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     TPO_CK_LAUNCH();
   } else {
-    k_precond_flat<double, double, PRE><<<update_flat_ctas(nx, ny), UF_THREADS, 0, st>>>(
+    k_precond_flat<double, double, PRE><<<flat_wave<k_precond_flat<double, double, PRE>>(nx, ny),
+                                            UF_THREADS, 0, st>>>(
         nx, ny, P, w.s64, w.mask, w.ra, w.z);
     TPO_CK_LAUNCH();
   }
@@ -627,7 +647,8 @@ int pcg_fp64(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, const
     if (block) {
       k_blockpre<double, double, false, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     } else {
-      k_update_flat<double, double, PRE><<<update_flat_ctas(nx, ny), UF_THREADS, 0, st>>>(up);
+      k_update_flat<double, double, PRE>
+          <<<flat_wave<k_update_flat<double, double, PRE>>(nx, ny), UF_THREADS, 0, st>>>(up);
     }
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
@@ -737,15 +758,16 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
 
   auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
-    StencilCfg<float, double, M_DIR, TPO_PRECOND_BLOCK_JACOBI>::launch(st, d, nx, ny);  // reads z
+    StencilCfg<float, float, M_DIR, TPO_PRECOND_BLOCK_JACOBI>::launch(st, d, nx, ny);  // reads z
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
     if (block) {
-      k_blockpre<float, double, false, kBlkL, double>
+      k_blockpre<float, float, false, kBlkL, double>
           <<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     } else {
-      k_update_flat<float, double, PRE, double><<<update_flat_ctas(nx, ny), UF_THREADS, 0, st>>>(up);
+      k_update_flat<float, float, PRE, double>
+          <<<flat_wave<k_update_flat<float, float, PRE, double>>(nx, ny), UF_THREADS, 0, st>>>(up);
     }
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
@@ -764,11 +786,12 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
     StencilCfg<double, double, M_RESX, PRE>::launch(st, rx, nx, ny);
     TPO_CK_LAUNCH();
     if (block) {
-      k_blockpre<float, double, true, kBlkL, double>
+      k_blockpre<float, float, true, kBlkL, double>
           <<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
       TPO_CK_LAUNCH();
     } else {  // z of the replaced residual (no-op when the replacement did not run)
-      k_precond_flat<float, double, PRE><<<update_flat_ctas(nx, ny), UF_THREADS, 0, st>>>(
+      k_precond_flat<float, float, PRE><<<flat_wave<k_precond_flat<float, float, PRE>>(nx, ny),
+                                          UF_THREADS, 0, st>>>(
           nx, ny, P, w.s32, w.mask, w.fra, w.fz);
       TPO_CK_LAUNCH();
     }

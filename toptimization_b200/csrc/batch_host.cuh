@@ -165,7 +165,7 @@ int filter_smem_bytes(int R) {
 
 template <int PRE> int batch_set_attrs() {
   constexpr int SMEM = StencilCfg<double, double, M_RESX, PRE>::SMEM;
-  constexpr int SMEM_D = StencilCfg<float, double, M_DIR, PRE>::SMEM;
+  constexpr int SMEM_D = StencilCfg<float, float, M_DIR, PRE>::SMEM;
   TPO_CK(cudaFuncSetAttribute(kb_resx<PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
   TPO_CK(cudaFuncSetAttribute(kb_dir<PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_D));
   TPO_CK(cudaFuncSetAttribute(kb_filter, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -242,7 +242,7 @@ template <int PRE>
 int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int use_h,
                bool cond = true, int steps = kBatchSteps) {
   constexpr int SMEM = StencilCfg<double, double, M_RESX, PRE>::SMEM;
-  constexpr int SMEM_D = StencilCfg<float, double, M_DIR, PRE>::SMEM;
+  constexpr int SMEM_D = StencilCfg<float, float, M_DIR, PRE>::SMEM;
   kb_resx<PRE><<<b->nctas[BK_STENCIL], TS_THREADS, SMEM, st>>>(
       jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs);
   TPO_CK_LAUNCH();

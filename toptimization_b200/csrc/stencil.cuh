@@ -70,6 +70,29 @@ __device__ __forceinline__ void elem_forces(T s, V2<T> bl, V2<T> br, V2<T> tr, V
   ftl = mk2<T>(-(PmQ + hx), RmQ - hy);
 }
 
+// elem_forces on x/y pairs: the same operations in the same order, issued as
+// two-wide arithmetic (packed FP32 instructions when T is float).
+template <typename T>
+__device__ __forceinline__ void elem_forces2(T s, V2<T> bl, V2<T> br, V2<T> tr, V2<T> tl,
+                                             V2<T> &fbl, V2<T> &fbr, V2<T> &ftr, V2<T> &ftl) {
+  const V2<T> A = sub2(tr, bl);  // (a, ay)
+  const V2<T> B = sub2(br, tl);  // (b, by)
+  const V2<T> S = add2(A, B);    // (a + b, ay + by)
+  const V2<T> D = sub2(A, B);    // (a - b, ay - by)
+  const T apb = S.x, ayb = D.y;
+  const V2<T> PR = mul2(bc2<T>(s), fma2(mk2<T>(kst<T>(0), kst<T>(1)), bc2<T>(apb),
+                                        mul2(mk2<T>(kst<T>(1), kst<T>(0)), bc2<T>(ayb))));
+  const T Q = s * kst<T>(2) * (D.x + S.y);
+  const V2<T> H = mul2(bc2<T>(s * kst<T>(3)), sub2(add2(bl, tr), add2(br, tl)));  // (hx, hy)
+  const V2<T> PQ = add2(PR, bc2<T>(Q));   // (P + Q, R + Q)
+  const V2<T> PmQ = sub2(PR, bc2<T>(Q));  // (P - Q, R - Q)
+  const V2<T> nH = mk2<T>(-H.x, -H.y);
+  fbl = sub2(H, PQ);
+  fbr = fma2(PmQ, mk2<T>(T(1), T(-1)), nH);
+  ftr = add2(PQ, H);
+  ftl = fma2(PmQ, mk2<T>(T(-1), T(1)), nH);
+}
+
 // Point preconditioners computed on the fly from the node's four element
 // scales (same argument order as node_apply).
 //  JACOBI: z = r / diag, diag_i = sum_e s_e Ke_ii, fixed -> 1, floor 1e-20
@@ -136,6 +159,10 @@ __device__ __forceinline__ double rcp_nr(double x) {
   e = fma(-x, y, 1.0);
   return fma(y, e, y);
 }
+// reciprocal in the preconditioner's arithmetic type: FP64 as above, FP32 the
+// correctly rounded single-precision reciprocal
+__device__ __forceinline__ double rcpT(double x) { return rcp_nr(x); }
+__device__ __forceinline__ float rcpT(float x) { return __frcp_rn(x); }
 
 // z = [[a, b], [b, d]] r: the point preconditioner of node (x, y) from its
 // four element scales (s_ll = (x-1,y-1), s_lh = (x-1,y), s_rl = (x,y-1),
@@ -160,8 +187,8 @@ __device__ __forceinline__ void node_pre(unsigned m, C s_ll, C s_lh, C s_rl, C s
     if constexpr (PRE == TPO_PRECOND_JACOBI) {
       if (m & FIXED_X) bxx = C(1); else if (bxx < C(1e-20)) bxx = C(1e-20);
       if (m & FIXED_Y) byy = C(1); else if (byy < C(1e-20)) byy = C(1e-20);
-      a = rcp_nr(bxx);
-      d = (byy == bxx) ? a : rcp_nr(byy);
+      a = rcpT(bxx);
+      d = (byy == bxx) ? a : rcpT(byy);
       b = C(0);
     } else {
       C bxy = kst<C>(5) * ((s_ll - s_lh) + (s_rh - s_rl));
@@ -169,7 +196,7 @@ __device__ __forceinline__ void node_pre(unsigned m, C s_ll, C s_lh, C s_rl, C s
       if (m & FIXED_Y) { byy = C(1); bxy = C(0); }
       const C det = bxx * byy - bxy * bxy;
       if (det > C(1e-36)) {
-        const C inv = rcp_nr(det);
+        const C inv = rcpT(det);
         a = byy * inv;
         d = bxx * inv;
         b = -bxy * inv;
