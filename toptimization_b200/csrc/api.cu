@@ -170,12 +170,18 @@ int sm_count() {
 // memory (set once), resident CTAs per SM, and the strip length that makes
 // the grid close to one full wave.
 #ifndef TPO_MIN_STRIP
-#define TPO_MIN_STRIP 16
+#define TPO_MIN_STRIP 8
+#endif
+#ifndef TPO_ST_G
+#define TPO_ST_G 2  // stencil columns per ring slot
+#endif
+#ifndef TPO_ST_NG
+#define TPO_ST_NG 4  // ring slots
 #endif
 constexpr int kMinStrip = TPO_MIN_STRIP;  // shortest stencil strip (node columns)
 template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
-  static constexpr int G = 2;
-  static constexpr int NG = 4;
+  static constexpr int G = TPO_ST_G;
+  static constexpr int NG = TPO_ST_NG;
   static constexpr int SMEM = TsGeom<T, MODE>::template slot_bytes<G>() * NG;
   static int resident() {
     static int occ = -1;
@@ -198,8 +204,6 @@ template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
     const int rows = (ny + 1 + RPC - 1) / RPC;
     const int target = sm_count() * resident();
     int strips = std::max(1, target / rows);
-    // a strip recomputes two columns besides its own: keep it long enough
-    // that the overlap stays small, even if the grid is then under one wave
     int L = std::max(kMinStrip, (nx + 1 + strips - 1) / strips);
     strips = (nx + 1 + L - 1) / L;
     return Plan{dim3(rows, strips, 1), L};
@@ -758,16 +762,16 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
 
   auto iter = [&](cudaEvent_t *ev) -> int {
     if (ev) TPO_CK(cudaEventRecord(ev[0], st));
-    StencilCfg<float, float, M_DIR, TPO_PRECOND_BLOCK_JACOBI>::launch(st, d, nx, ny);  // reads z
+    StencilCfg<float, double, M_DIR, TPO_PRECOND_BLOCK_JACOBI>::launch(st, d, nx, ny);  // reads z
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
     if (block) {
-      k_blockpre<float, float, false, kBlkL, double>
+      k_blockpre<float, double, false, kBlkL, double>
           <<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
     } else {
-      k_update_flat<float, float, PRE, double>
-          <<<flat_wave<k_update_flat<float, float, PRE, double>>(nx, ny), UF_THREADS, 0, st>>>(up);
+      k_update_flat<float, double, PRE, double>
+          <<<flat_wave<k_update_flat<float, double, PRE, double>>(nx, ny), UF_THREADS, 0, st>>>(up);
     }
     TPO_CK_LAUNCH();
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
@@ -786,11 +790,11 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
     StencilCfg<double, double, M_RESX, PRE>::launch(st, rx, nx, ny);
     TPO_CK_LAUNCH();
     if (block) {
-      k_blockpre<float, float, true, kBlkL, double>
+      k_blockpre<float, double, true, kBlkL, double>
           <<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
       TPO_CK_LAUNCH();
     } else {  // z of the replaced residual (no-op when the replacement did not run)
-      k_precond_flat<float, float, PRE><<<flat_wave<k_precond_flat<float, float, PRE>>(nx, ny),
+      k_precond_flat<float, double, PRE><<<flat_wave<k_precond_flat<float, double, PRE>>(nx, ny),
                                           UF_THREADS, 0, st>>>(
           nx, ny, P, w.s32, w.mask, w.fra, w.fz);
       TPO_CK_LAUNCH();

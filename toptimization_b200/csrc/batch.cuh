@@ -126,6 +126,9 @@ __global__ void kb_mark(BDesign *ds, int n) {
   if (st != TPO_SOLVE_RUNNING && st != SOLVE_NEED_UPDATE) D.phase = PH_POST;
 }
 
+// stencil ring of the batched kernels: kBatchNG slots of kBatchG columns
+constexpr int kBatchG = 2, kBatchNG = 4;
+
 template <int PRE>
 __global__ void __launch_bounds__(TS_THREADS) kb_resx(const BJob *jobs, int nj, const BDesign *ds) {
   const BJob &J = find_job(jobs, nj);
@@ -146,7 +149,7 @@ __global__ void __launch_bounds__(TS_THREADS) kb_resx(const BJob *jobs, int nj, 
   a.octl = D.octl;
   a.err = &D.ctl->err;
   const int loc = blockIdx.x - J.cta0;
-  tstencil_run<double, double, M_RESX, PRE, 2, 4>(a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy,
+  tstencil_run<double, double, M_RESX, PRE, kBatchG, kBatchNG>(a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy,
                                                   loc);
 }
 
@@ -169,7 +172,7 @@ __global__ void __launch_bounds__(TS_THREADS) kb_dir(const BJob *jobs, int nj, c
   a.ctl = D.ctl;
   a.err = &D.ctl->err;
   const int loc = blockIdx.x - J.cta0;
-  tstencil_run<float, float, M_DIR, TPO_PRECOND_BLOCK_JACOBI, 2, 4>(
+  tstencil_run<float, double, M_DIR, TPO_PRECOND_BLOCK_JACOBI, kBatchG, kBatchNG>(
       a, J.L, loc % J.gx, loc / J.gx, J.gx * J.gy, loc);
 }
 
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(UF_THREADS) kb_pre(const BJob *jobs, int nj, c
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
   if (!D.active || D.phase != PH_SOLVE || D.ctl->status != TPO_SOLVE_RUNNING) return;
-  precond_flat_run<float, float, PRE>(D.nx, D.ny, D.P, D.s32, D.mask, D.fr, D.fz,
+  precond_flat_run<float, double, PRE>(D.nx, D.ny, D.P, D.s32, D.mask, D.fr, D.fz,
                                        blockIdx.x - J.cta0, J.gx);
 }
 
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(UF_THREADS) kb_update(const BJob *jobs, int nj
   a.ctl = D.ctl;
   a.z = D.fz;
   const int loc = blockIdx.x - J.cta0;
-  update_flat_run<float, float, PRE, double>(a, loc, J.gx, J.gx, loc);
+  update_flat_run<float, double, PRE, double>(a, loc, J.gx, J.gx, loc);
 }
 
 // Is any solve of the batch still going? flag[0] = 1 if so; flag[1] = 1 when

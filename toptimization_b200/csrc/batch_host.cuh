@@ -164,8 +164,8 @@ int filter_smem_bytes(int R) {
 }
 
 template <int PRE> int batch_set_attrs() {
-  constexpr int SMEM = StencilCfg<double, double, M_RESX, PRE>::SMEM;
-  constexpr int SMEM_D = StencilCfg<float, float, M_DIR, PRE>::SMEM;
+  constexpr int SMEM = TsGeom<double, M_RESX>::template slot_bytes<kBatchG>() * kBatchNG;
+  constexpr int SMEM_D = TsGeom<float, M_DIR>::template slot_bytes<kBatchG>() * kBatchNG;
   TPO_CK(cudaFuncSetAttribute(kb_resx<PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
   TPO_CK(cudaFuncSetAttribute(kb_dir<PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_D));
   TPO_CK(cudaFuncSetAttribute(kb_filter, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -241,8 +241,8 @@ int batch_prefix(tpo_batch *b, cudaStream_t st) {
 template <int PRE>
 int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int use_h,
                bool cond = true, int steps = kBatchSteps) {
-  constexpr int SMEM = StencilCfg<double, double, M_RESX, PRE>::SMEM;
-  constexpr int SMEM_D = StencilCfg<float, float, M_DIR, PRE>::SMEM;
+  constexpr int SMEM = TsGeom<double, M_RESX>::template slot_bytes<kBatchG>() * kBatchNG;
+  constexpr int SMEM_D = TsGeom<float, M_DIR>::template slot_bytes<kBatchG>() * kBatchNG;
   kb_resx<PRE><<<b->nctas[BK_STENCIL], TS_THREADS, SMEM, st>>>(
       jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs);
   TPO_CK_LAUNCH();

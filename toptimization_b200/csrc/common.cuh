@@ -68,29 +68,6 @@ template <typename T> __device__ __forceinline__ V2<T> shfl_down2(V2<T> v) {
   return mk2<T>(__shfl_down_sync(FULL, v.x, 1), __shfl_down_sync(FULL, v.y, 1));
 }
 
-// Two-wide arithmetic on an x/y pair. FP32 pairs use sm_100's packed FP32
-// instructions (one FFMA2 / FADD2 / FMUL2 per pair); FP64 pairs are two
-// scalar operations.
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
-  return __fadd2_rn(a, make_float2(-b.x, -b.y));
-}
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ double2 add2(double2 a, double2 b) {
-  return make_double2(a.x + b.x, a.y + b.y);
-}
-__device__ __forceinline__ double2 sub2(double2 a, double2 b) {
-  return make_double2(a.x - b.x, a.y - b.y);
-}
-__device__ __forceinline__ double2 mul2(double2 a, double2 b) {
-  return make_double2(a.x * b.x, a.y * b.y);
-}
-__device__ __forceinline__ double2 fma2(double2 a, double2 b, double2 c) {
-  return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
-}
-template <typename T> __device__ __forceinline__ V2<T> bc2(T v) { return mk2<T>(v, v); }
-
 // FP64 dot of two pairs (products of FP32 values are exact in FP64)
 template <typename A, typename B>
 __device__ __forceinline__ double dot2d(A a, B b) {

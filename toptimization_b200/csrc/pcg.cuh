@@ -14,25 +14,22 @@
 //
 // T is the storage type of the Krylov vectors (r, p, Ap, z) and scales, C the
 // arithmetic type, X the type of the solution u: <double,double,double> for
-// the plain FP64 solve, <float,float,double> for the mixed form (FP32 bytes
-// and FP32 arithmetic for the matvec, the preconditioner and the vector
-// updates; FP64 for the dot products, alpha/beta and the solution). u stays
+// the plain FP64 solve, <float,double,double> for the mixed form (FP32 bytes
+// for the Krylov vectors, FP64 arithmetic, dot products and solution). u stays
 // FP64 in the mixed form: accumulating it in FP32 between residual
 // replacements injects rounding noise of relative size 2^-24 into every
 // replaced residual, which the iteration then has to remove again.
 //
-// k_tstencil: each CTA owns 120 grid rows and walks a strip of L node
-// columns. Column windows of every input are staged into shared memory by TMA
-// bulk copies (cp.async.bulk) in groups of G columns, NG groups in flight,
-// completion on one mbarrier per ring slot; one warp produces, one consumes.
-// A consumer lane holds four consecutive rows (lanes 0..30 cover rows
-// Y0-2 .. Y0+121), so the elements between its rows need no shuffle: per
-// column only the node above its last row and the forces of the element below
-// its first row cross lanes. Element arithmetic is issued on x/y pairs
-// (packed FP32 instructions in the mixed form). Strips overlap by two
-// columns; values there are recomputed from the inputs, never read from
-// another strip's output, and the direction p ping-pongs between two buffers
-// so no CTA overwrites what another still reads.
+// k_tstencil: each CTA owns 120 grid rows (4 warps x 30; a warp's first and
+// last lane are halo rows) and walks a strip of L node columns. Column windows
+// of every input are staged into shared memory by TMA bulk copies
+// (cp.async.bulk) in groups of G columns, NG groups in flight, completion on
+// one mbarrier per ring slot; a fifth warp produces, four warps consume. Each
+// thread keeps the 3x3 neighbourhood of transformed nodal values in registers,
+// y neighbours arrive by warp shuffles. Strips overlap by two columns; values
+// there are recomputed from the inputs, never read from another strip's
+// output, and the direction p ping-pongs between two buffers so no CTA
+// overwrites what another still reads.
 #pragma once
 
 #include "common.cuh"
@@ -42,13 +39,7 @@
 namespace tpo {
 
 constexpr int ST_THREADS = WPC * 32;  // 128 (k_blockpre)
-// Stencil CTA: one consumer warp whose lanes hold LR consecutive grid rows
-// each (lanes 0..30 cover rows Y0-2 .. Y0+121, the staged node window; lane 31
-// mirrors lane 30 and its results are discarded), and one producer warp.
-constexpr int LR = 4;
-constexpr int TS_LANES = 31;
-constexpr int TS_THREADS = 64;
-static_assert(LR * TS_LANES == N_WIN, "the consumer lanes cover the staged node window");
+constexpr int TS_THREADS = ST_THREADS + 32;  // stencil: 4 consumer warps + 1 producer warp
 
 enum StMode { M_RAW = 0, M_DIR = 1, M_RES = 2, M_RESX = 3 };
 
@@ -88,81 +79,6 @@ template <typename T, int MODE> struct TsGeom {
   }
 };
 
-// LR consecutive nodal pairs of a staged column from window index i0
-// (a multiple of LR: 16-byte aligned for both storage types)
-template <typename T>
-__device__ __forceinline__ void lds_pairs(const V2<T> *col, int i0, V2<T> (&v)[LR]) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 a = *reinterpret_cast<const float4 *>(col + i0);
-    const float4 b = *reinterpret_cast<const float4 *>(col + i0 + 2);
-    v[0] = make_float2(a.x, a.y);
-    v[1] = make_float2(a.z, a.w);
-    v[2] = make_float2(b.x, b.y);
-    v[3] = make_float2(b.z, b.w);
-  } else {
-#pragma unroll
-    for (int j = 0; j < LR; ++j) v[j] = col[i0 + j];
-  }
-}
-
-// Element scales of a staged column at rows yb-1 .. yb+LR-1, e0 = the window
-// index of row yb. The float window holds row yb-1 for every lane; in the
-// double window lane 0's row yb-1 (= Y0-3) is not staged: it is only used for
-// the preconditioner of row Y0-2, which is no output row, so the index is
-// clamped to stay inside the window.
-template <typename T>
-__device__ __forceinline__ void lds_scales(const T *col, int e0, T (&s)[LR + 1]) {
-  if constexpr (sizeof(T) == 4) {  // e0 = 2 (mod 4)
-    s[0] = col[e0 - 1];
-    const float2 a = *reinterpret_cast<const float2 *>(col + e0);
-    const float2 b = *reinterpret_cast<const float2 *>(col + e0 + 2);
-    s[1] = a.x;
-    s[2] = a.y;
-    s[3] = b.x;
-    s[4] = b.y;
-  } else {  // e0 = 0 (mod 4)
-    s[0] = col[e0 > 0 ? e0 - 1 : 0];
-    const double2 a = *reinterpret_cast<const double2 *>(col + e0);
-    const double2 b = *reinterpret_cast<const double2 *>(col + e0 + 2);
-    s[1] = a.x;
-    s[2] = a.y;
-    s[3] = b.x;
-    s[4] = b.y;
-  }
-}
-
-// the four fixed-mask bytes of rows yb .. yb+3 (byte j = row yb+j), i0 = 2 (mod 4)
-__device__ __forceinline__ unsigned lds_mask4(const uint8_t *col, int i0) {
-  const unsigned lo = *reinterpret_cast<const uint16_t *>(col + i0);
-  const unsigned hi = *reinterpret_cast<const uint16_t *>(col + i0 + 2);
-  return lo | (hi << 16);
-}
-
-// Store the pairs of rows j with bit j of `own` set, from slot0 (a multiple of
-// two slots: 16-byte aligned for FP32 pairs). Whole 16-byte runs go out as one
-// vector store.
-template <typename T>
-__device__ __forceinline__ void stg_pairs(T *base, size_t slot0, const V2<T> (&v)[LR],
-                                          unsigned own) {
-  V2<T> *p = reinterpret_cast<V2<T> *>(base) + slot0;
-  if constexpr (sizeof(T) == 4) {
-#pragma unroll
-    for (int h = 0; h < LR; h += 2) {
-      const unsigned two = (own >> h) & 3u;
-      if (two == 3u)
-        *reinterpret_cast<float4 *>(p + h) = make_float4(v[h].x, v[h].y, v[h + 1].x, v[h + 1].y);
-      else if (two == 1u)
-        p[h] = v[h];
-      else if (two == 2u)
-        p[h + 1] = v[h + 1];
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < LR; ++j)
-      if ((own >> j) & 1u) p[j] = v[j];
-  }
-}
-
 // (bx, by) = (row block, strip) of this CTA, nb / bid = CTAs of the solve and
 // this CTA's index among them (a batched launch runs many solves at once)
 template <typename T, typename C, int MODE, int PRE, int G, int NG>
@@ -190,16 +106,19 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     // (or before the first iteration): a batched launch reaches every solve
     if (ctl->status != SOLVE_NEED_UPDATE || a.octl->status != TPO_SOLVE_RUNNING) return;
   }
-  // the direction kernel reads z = M r as stored by the update kernel (or
-  // the element-block preconditioner); it never rebuilds a preconditioner
-  static_assert(MODE != M_DIR || PRE == TPO_PRECOND_BLOCK_JACOBI, "DIR reads the stored z");
   const int nx = a.nx, ny = a.ny, P = a.P;
   const int Y0 = bx * RPC;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int y = Y0 + wid * RPW - 1 + lane;
+  const bool own_row = lane >= 1 && lane <= RPW && y <= ny;
   const int x0 = by * L;
   const int x1 = min(x0 + L, nx + 1);
-  const int cA = x0 - 1;       // first staged column
-  const int NC = x1 - cA + 1;  // staged columns cA..x1
+  // Only a direction kernel that rebuilds a point preconditioner at node
+  // x0-1 needs element column x0-2: it stages that column's scales alone.
+  // Every other mode starts at x0-1 with nodes and scales.
+  constexpr bool SCALE_COL = MODE == M_DIR && PRE != TPO_PRECOND_BLOCK_JACOBI;
+  const int cA = x0 - (SCALE_COL ? 2 : 1);  // first staged column
+  const int NC = x1 - cA + 1;               // staged columns cA..x1
   const int NGRP = (NC + G - 1) / G;
   const int ms = (Y0 + LEAD - 1) & ~15;  // first staged mask byte of a column
 
@@ -211,22 +130,25 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     dst_p = static_cast<T *>(parity ? a.pa : a.pb);
   }
 
-  // ---- producer: stage group g into ring slot g % NG. A slot is reused only
-  // after the consumer warp has released the group it held (empty[]).
+  // ---- producer (thread 0): stage group g into ring slot g % NG. A slot is
+  // reused only after every warp has released the group it held (empty[]),
+  // and the producer refills with a lag of one group, so warps may drift
+  // apart by a group without waiting for each other.
   auto issue = [&](int g) {
     unsigned char *sb = smem + (g % NG) * SLOT;
     unsigned bytes = 0;
     for (int k = 0; k < G; ++k) {
       const int c = cA + g * G + k;
       if (c > x1) break;
-      if (c >= 0 && c <= nx) bytes += Geo::CNB * (Geo::HAS_B ? 2 : 1) + Geo::CMB;
+      if ((!SCALE_COL || c > cA) && c >= 0 && c <= nx)
+        bytes += Geo::CNB * (Geo::HAS_B ? 2 : 1) + Geo::CMB;
       if (c >= 0 && c < nx) bytes += Geo::CEB;
     }
     mbar_arrive_expect_tx(&full[g % NG], bytes);
     for (int k = 0; k < G; ++k) {
       const int c = cA + g * G + k;
       if (c > x1) break;
-      if (c >= 0 && c <= nx) {
+      if ((!SCALE_COL || c > cA) && c >= 0 && c <= nx) {
         const size_t col = (size_t)c * P + Y0 + N_OFF;
         bulk_g2s(sb + k * Geo::CNB, ga + 2 * col, Geo::CNB, &full[g % NG]);
         if constexpr (Geo::HAS_B)
@@ -244,7 +166,7 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
   if (threadIdx.x == 0) {
     for (int s = 0; s < NG; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+      mbar_init(&empty[s], WPC);
     }
     fence_mbar_init();
   }
@@ -253,7 +175,7 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = 0.0;
 
-  if (wid == 1) {
+  if (wid == WPC) {
     // ---- producer warp: refill slot g % NG with group g once its previous
     // tenant (g - NG) has been released by every consumer warp
     if (lane == 0) {
@@ -271,41 +193,20 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     }
   } else {
 
-  // Lane l holds rows yb + j, j = 0..LR-1, yb = Y0 - 2 + LR l: node window
-  // index LR l + j, element window index LR l + j + EOFF (EOFF = rows of the
-  // element window below row Y0 - 2), mask byte m0 + j. Lane 31 reads lane
-  // 30's rows (its results are discarded). Rows Y0 .. Y0 + RPC - 1 (and
-  // <= ny) are this CTA's output rows.
-  const int lq = min(lane, TS_LANES - 1);
-  const int yb = Y0 - 2 + LR * lane;
-  const int n0 = LR * lq;
-  constexpr int EOFF = LEAD - 2 - EWin<T>::OFF;  // float: 2, double: 0
-  const int e0 = n0 + EOFF;                       // element row yb (row yb - 1 is e0 - 1)
-  const int m0 = Y0 + LEAD - 2 + n0 - ms;         // 2 (mod 4): u16-aligned
-  unsigned own = 0;  // bit j: row yb + j is an output row of this CTA
-#pragma unroll
-  for (int j = 0; j < LR; ++j) {
-    const int yj = yb + j;
-    if (lane < TS_LANES && yj >= Y0 && yj < Y0 + RPC && yj <= ny) own |= 1u << j;
-  }
+  // per-lane indices inside the staged column windows
+  const int n_idx = y - Y0 + 2;
+  const int e_idx = y - Y0 + (LEAD - 1 - EWin<T>::OFF);  // element row y-1; row y is +1
+  const int m_idx = y + LEAD - ms;
 
-  // Element-centric march along x. At step c the lane transforms its nodes
-  // (c, yb+j) (p_new, or u with fixed DOFs zeroed), forms elements
-  // (c-1, yb+j) from their corners (c-1, y) (c, y) (c, y+1) (c-1, y+1), and
-  // finishes nodes (c-1, yb+j): carry[j] holds what elements (c-2, y) and
-  // (c-2, y-1) gave node (c-1, y) one step earlier. The node above the lane's
-  // last row comes from the next lane, the forces of the element below its
-  // first row from the previous lane (two shuffles of pairs per column).
+  // Element-centric march. At step c lane y transforms node (c, y) (p_new,
+  // or u with fixed DOFs zeroed), forms element (c-1, y) from its corners
+  // (c-1, y) (c, y) (c, y+1) (c-1, y+1), and finishes node (c-1, y): the carry
+  // holds what elements (c-2, y) and (c-2, y-1) gave it one step earlier.
   const V2<C> zero2 = mk2<C>(C(0), C(0));
-  V2<C> vp[LR + 1], carry[LR];
-  C sp[LR + 1], sq[LR + 1];  // element columns c-1 and c-2, rows yb-1 .. yb+LR-1
-  unsigned mp = 0;           // fixed-mask bytes of node column c-1 (byte j: row yb+j)
-#pragma unroll
-  for (int j = 0; j <= LR; ++j) {
-    vp[j] = zero2;
-    sp[j] = sq[j] = C(0);
-    if (j < LR) carry[j] = zero2;
-  }
+  V2<C> pn_prev = zero2, pu_prev = zero2, carry = zero2;
+  C sprev_d = C(0), sprev_u = C(0);  // element column c-1, rows y-1, y
+  C s2_d = C(0), s2_u = C(0);        // element column c-2, rows y-1, y (residual modes)
+  unsigned m_prev = 0;
 
   for (int k = 0; k < NC; ++k) {
     const int c = cA + k;
@@ -317,152 +218,102 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
     const T *colS = reinterpret_cast<const T *>(sb + G * Geo::CNB * (Geo::HAS_B ? 2 : 1) +
                                                 kk * Geo::CEB);
     const uint8_t *colM = sb + G * Geo::CNB * (Geo::HAS_B ? 2 : 1) + G * Geo::CEB + kk * Geo::CMB;
-    const bool node_ok = c >= 0 && c <= nx;
+    const bool node_ok = (!SCALE_COL || c > cA) && c >= 0 && c <= nx;
     const bool elem_ok = c >= 0 && c < nx;
+    const C scd = elem_ok ? C(colS[e_idx]) : C(0);      // element (c, y-1)
+    const C scu = elem_ok ? C(colS[e_idx + 1]) : C(0);  // element (c, y)
 
-    // ---- element scales of column c, rows yb-1 .. yb+LR-1
-    C sc[LR + 1];
-    if (elem_ok) {
-      T sv[LR + 1];
-      lds_scales<T>(colS, e0, sv);
-#pragma unroll
-      for (int j = 0; j <= LR; ++j) sc[j] = C(sv[j]);
-    } else {
-#pragma unroll
-      for (int j = 0; j <= LR; ++j) sc[j] = C(0);
-    }
-
-    // ---- transformed nodal values at (c, yb+j)
-    V2<C> v[LR + 1];
-    unsigned mc = 0;
+    // ---- transformed nodal value at (c, y)
+    V2<C> v = zero2;
+    const unsigned m = node_ok ? colM[m_idx] : 0u;
     if (node_ok) {
-      mc = lds_mask4(colM, m0);
-      V2<T> av[LR];
-      lds_pairs<T>(colA, n0, av);
-      if constexpr (MODE == M_DIR) {
+      const V2<C> av = cvt2<C, T>(colA[n_idx]);
+      if constexpr (MODE == M_RAW) {
+        v = av;
+      } else if constexpr (MODE == M_DIR) {
+        V2<C> z;
+        if constexpr (PRE == TPO_PRECOND_BLOCK_JACOBI) z = av;
+        else z = point_precond<C, PRE>(av, m, sprev_d, sprev_u, scd, scu);
         if (first) {
-#pragma unroll
-          for (int j = 0; j < LR; ++j) v[j] = cvt2<C, T>(av[j]);
+          v = z;
         } else {
-          V2<T> po[LR];
-          lds_pairs<T>(colB, n0, po);
-#pragma unroll
-          for (int j = 0; j < LR; ++j)
-            v[j] = fma2(bc2<C>(beta), cvt2<C, T>(po[j]), cvt2<C, T>(av[j]));
+          const V2<C> po = cvt2<C, T>(colB[n_idx]);
+          v = mk2<C>(fmaT(beta, po.x, z.x), fmaT(beta, po.y, z.y));
         }
-#pragma unroll
-        for (int j = 0; j < LR; ++j)  // the stored direction is what K sees
-          v[j] = cvt2<C, T>(mk2<T>(T(v[j].x), T(v[j].y)));
-      } else {
-#pragma unroll
-        for (int j = 0; j < LR; ++j) v[j] = cvt2<C, T>(av[j]);
-        if constexpr (MODE == M_RES || MODE == M_RESX) {
-          // u with fixed DOFs zeroed (idempotent write-back on owned nodes)
-#pragma unroll
-          for (int j = 0; j < LR; ++j) {
-            const unsigned m = (mc >> (8 * j)) & 0xffu;
-            if (m & FIXED_X) v[j].x = C(0);
-            if (m & FIXED_Y) v[j].y = C(0);
-            if (m && ((own >> j) & 1u) && c >= x0 && c < x1)
-              st2<T>(static_cast<T *>(a.uw), pslot(c, yb + j, P), mk2<T>(T(v[j].x), T(v[j].y)));
-          }
-        }
+        v = cvt2<C, T>(mk2<T>(T(v.x), T(v.y)));  // the stored direction is what K sees
+      } else {  // M_RES, M_RESX: u with fixed DOFs zeroed (idempotent write-back)
+        v = av;
+        if (m & FIXED_X) v.x = C(0);
+        if (m & FIXED_Y) v.y = C(0);
+        if (m && own_row && c >= x0 && c < x1)
+          st2<T>(static_cast<T *>(a.uw), pslot(c, y, P), mk2<T>(T(v.x), T(v.y)));
       }
-    } else {
-#pragma unroll
-      for (int j = 0; j < LR; ++j) v[j] = zero2;
     }
-    v[LR] = shfl_down2<C>(v[0]);  // node (c, yb+LR)
+    const V2<C> vu = shfl_down2<C>(v);  // node (c, y+1)
 
-    // ---- elements (c-1, yb+j): corners (c-1,y) (c,y) (c,y+1) (c-1,y+1)
-    V2<C> fbl[LR], fbr[LR], ftr[LR], ftl[LR];
-#pragma unroll
-    for (int j = 0; j < LR; ++j)
-      elem_forces2<C>(sp[j + 1], vp[j], v[j], v[j + 1], vp[j + 1], fbl[j], fbr[j], ftr[j], ftl[j]);
-    const V2<C> tl_below = shfl_up2<C>(ftl[LR - 1]);  // element (c-1, yb-1) -> node (c-1, yb)
-    const V2<C> tr_below = shfl_up2<C>(ftr[LR - 1]);  // element (c-1, yb-1) -> node (c, yb)
+    // ---- element (c-1, y): corners (c-1,y) (c,y) (c,y+1) (c-1,y+1)
+    V2<C> fbl, fbr, ftr, ftl;
+    elem_forces<C>(sprev_u, pn_prev, v, vu, pu_prev, fbl, fbr, ftr, ftl);
+    const V2<C> tl_below = shfl_up2<C>(ftl);  // element (c-1, y-1) -> node (c-1, y)
+    const V2<C> tr_below = shfl_up2<C>(ftr);  // element (c-1, y-1) -> node (c, y)
 
-    // the consumer is done with group g: release its slot to the producer
-    if (kk == G - 1 || k == NC - 1) {
+    // this warp is done with group g: release it; thread 0 then stages
+    // group g + NG - 1 into the slot of group g - 1
+    if (kk == G - 1 || k == NC - 1) {  // group done: release it to the producer
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[g % NG]);
     }
 
-    // ---- nodes (xo, yb+j), xo = c - 1, are complete
+    // ---- node (xo, y), xo = c - 1, is complete
     const int xo = c - 1;
-    if (own && xo >= x0) {
-      const size_t node0 = pslot(xo, yb, P);
-      V2<C> kv[LR];
-#pragma unroll
-      for (int j = 0; j < LR; ++j) {
-        kv[j] = add2(add2(carry[j], fbl[j]), j ? ftl[j - 1] : tl_below);
-        const unsigned m = (mp >> (8 * j)) & 0xffu;
-        if (m & FIXED_X) kv[j].x = vp[j].x;  // identity rows at fixed DOFs
-        if (m & FIXED_Y) kv[j].y = vp[j].y;
-      }
-      if constexpr (MODE == M_RAW || MODE == M_DIR) {
-        V2<T> ks[LR];
-#pragma unroll
-        for (int j = 0; j < LR; ++j) {
-          ks[j] = mk2<T>(T(kv[j].x), T(kv[j].y));
-          if ((own >> j) & 1u) acc[0] += dot2d(vp[j], ks[j]);
-        }
-        if constexpr (MODE == M_DIR) {
-          V2<T> pt[LR];
-#pragma unroll
-          for (int j = 0; j < LR; ++j) pt[j] = mk2<T>(T(vp[j].x), T(vp[j].y));
-          stg_pairs<T>(dst_p, node0, pt, own);
-        }
-        stg_pairs<T>(static_cast<T *>(a.out), node0, ks, own);
+    if (own_row && xo >= x0) {
+      const size_t node = pslot(xo, y, P);
+      V2<C> kv = mk2<C>(carry.x + fbl.x + tl_below.x, carry.y + fbl.y + tl_below.y);
+      if (m_prev & FIXED_X) kv.x = pn_prev.x;  // identity rows at fixed DOFs
+      if (m_prev & FIXED_Y) kv.y = pn_prev.y;
+      if constexpr (MODE == M_RAW) {
+        const V2<T> ks = mk2<T>(T(kv.x), T(kv.y));
+        st2<T>(static_cast<T *>(a.out), node, ks);
+        acc[0] += (double)pn_prev.x * (double)ks.x + (double)pn_prev.y * (double)ks.y;
+      } else if constexpr (MODE == M_DIR) {
+        const V2<T> ks = mk2<T>(T(kv.x), T(kv.y));
+        st2<T>(dst_p, node, mk2<T>(T(pn_prev.x), T(pn_prev.y)));
+        st2<T>(static_cast<T *>(a.out), node, ks);
+        acc[0] += (double)pn_prev.x * (double)ks.x + (double)pn_prev.y * (double)ks.y;
       } else if constexpr (MODE == M_RES) {
-        V2<T> rs[LR];
-#pragma unroll
-        for (int j = 0; j < LR; ++j) {
-          rs[j] = mk2<T>(T(0), T(0));
-          if (!((own >> j) & 1u)) continue;
-          const V2<C> f = cvt2<C, T>(ld2<T>(static_cast<const T *>(a.f), node0 + j));
-          rs[j] = mk2<T>(T(f.x - kv[j].x), T(f.y - kv[j].y));
-          if constexpr (PRE != TPO_PRECOND_BLOCK_JACOBI) {
-            C pa, pb, pd;
-            node_pre<C, PRE>((mp >> (8 * j)) & 0xffu, sq[j], sq[j + 1], sp[j], sp[j + 1], pa, pb,
-                             pd);
-            acc[0] += dot2d(rs[j], pre_apply<C>(pa, pb, pd, cvt2<C, T>(rs[j])));
-          }
-          acc[1] += dot2d(rs[j], rs[j]);
+        const V2<C> f = cvt2<C, T>(ld2<T>(static_cast<const T *>(a.f), node));
+        const V2<T> r = mk2<T>(T(f.x - kv.x), T(f.y - kv.y));
+        st2<T>(static_cast<T *>(a.out), node, r);
+        if constexpr (PRE != TPO_PRECOND_BLOCK_JACOBI) {
+          const V2<C> z = point_precond<C, PRE>(cvt2<C, T>(r), m_prev, s2_d, s2_u, sprev_d,
+                                                sprev_u);
+          acc[0] += (double)r.x * z.x + (double)r.y * z.y;
         }
-        stg_pairs<T>(static_cast<T *>(a.out), node0, rs, own);
-      } else {  // M_RESX: T == C == double; the inner solve stores FP32 and runs in FP32
-        float2 r32[LR];
-#pragma unroll
-        for (int j = 0; j < LR; ++j) {
-          r32[j] = make_float2(0.f, 0.f);
-          if (!((own >> j) & 1u)) continue;
-          const double2 f = ld2<double>(static_cast<const double *>(a.f), node0 + j);
-          const double rx = f.x - (double)kv[j].x, ry = f.y - (double)kv[j].y;
-          acc[0] += rx * rx + ry * ry;
-          r32[j] = make_float2((float)rx, (float)ry);
-          if constexpr (PRE != TPO_PRECOND_BLOCK_JACOBI) {
-            // the inner z = M r, formed as the inner kernels form it (FP32
-            // scales and arithmetic)
-            float pa, pb, pd;
-            node_pre<float, PRE>((mp >> (8 * j)) & 0xffu, (float)sq[j], (float)sq[j + 1],
-                                 (float)sp[j], (float)sp[j + 1], pa, pb, pd);
-            acc[1] += dot2d(r32[j], pre_apply<float>(pa, pb, pd, r32[j]));
-          }
-          acc[2] += dot2d(r32[j], r32[j]);
+        acc[1] += (double)r.x * r.x + (double)r.y * r.y;
+      } else {  // M_RESX: T == C == double; the inner solve stores float
+        const double2 f = ld2<double>(static_cast<const double *>(a.f), node);
+        const double rx = f.x - (double)kv.x, ry = f.y - (double)kv.y;
+        acc[0] += rx * rx + ry * ry;
+        const float2 r32 = make_float2((float)rx, (float)ry);
+        st2<float>(static_cast<float *>(a.out), node, r32);
+        if constexpr (PRE != TPO_PRECOND_BLOCK_JACOBI) {
+          // the inner kernels see FP32-stored scales: use the same here
+          const double2 z = point_precond<double, PRE>(
+              make_double2(r32.x, r32.y), m_prev, (double)(float)s2_d, (double)(float)s2_u,
+              (double)(float)sprev_d, (double)(float)sprev_u);
+          acc[1] += (double)r32.x * z.x + (double)r32.y * z.y;
         }
-        stg_pairs<float>(static_cast<float *>(a.out), node0, r32, own);
+        acc[2] += (double)r32.x * r32.x + (double)r32.y * r32.y;
       }
     }
-#pragma unroll
-    for (int j = 0; j < LR; ++j) carry[j] = add2(fbr[j], j ? ftr[j - 1] : tr_below);
-#pragma unroll
-    for (int j = 0; j <= LR; ++j) {
-      vp[j] = v[j];
-      sq[j] = sp[j];
-      sp[j] = sc[j];
-    }
-    mp = mc;
+    carry = mk2<C>(fbr.x + tr_below.x, fbr.y + tr_below.y);
+    pn_prev = v;
+    pu_prev = vu;
+    s2_d = sprev_d;
+    s2_u = sprev_u;
+    sprev_d = scd;
+    sprev_u = scu;
+    m_prev = m;
   }
 
   }  // consumer warps
@@ -566,16 +417,20 @@ __device__ __forceinline__ void finish_update(PcgCtl *ctl, double rz_new, double
 
 
 // Same update, pointwise over the grid's nodes with a flat grid-stride loop.
-// A thread takes UQ = 4 consecutive rows of one node column per pass, so
-// every vector arrives as 16-byte loads (two per FP32 run of four nodes,
-// four per FP64 run) and a thread has about 200 bytes in flight; no column
-// walk. The node's four element scales come straight from the padded scale
-// array: element (c-1, y-1), (c-1, y), (c, y-1), (c, y) sit at the node's
-// slot - P - 1, - P, - 1 and + 0 (zero pads outside the grid rows). Only grid
-// rows are written and summed.
+// A warp takes runs of RUN = 32 UQ consecutive grid nodes (the compact
+// numbering, column after column); lane l holds nodes base + l + 32 j,
+// j < UQ, so every load and store instruction of the warp covers 32
+// consecutive nodes (one break per column boundary), and all UQ nodes' loads
+// are issued before any is used. The node's four element scales come
+// straight from the padded scale array: element (c-1, y-1), (c-1, y),
+// (c, y-1), (c, y) sit at the node's slot - P - 1, - P, - 1 and + 0 (zero
+// pads outside the grid rows).
 constexpr int UF_THREADS = 256;
-constexpr int UQ = 4;
-static_assert(UQ == LR, "the run stores reuse stg_pairs");
+#ifndef TPO_UQ
+#define TPO_UQ 1
+#endif
+constexpr int UQ = TPO_UQ;  // nodes per lane and pass
+constexpr int RUN = 32 * UQ;
 
 // n / d for 0 <= n < 2^31 through a double reciprocal, corrected to exact
 __device__ __forceinline__ int div_exact(int n, int d, double inv_d) {
@@ -585,47 +440,44 @@ __device__ __forceinline__ int div_exact(int n, int d, double inv_d) {
   return q;
 }
 
-// the nodal pairs of slots s0 .. s0+3 (s0 a multiple of 4: 32-byte aligned)
-template <typename T>
-__device__ __forceinline__ void ldg_quad(const T *__restrict__ base, size_t s0, V2<T> (&v)[UQ]) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 *q = reinterpret_cast<const float4 *>(base + 2 * s0);
-    const float4 a = q[0], b = q[1];
-    v[0] = make_float2(a.x, a.y);
-    v[1] = make_float2(a.z, a.w);
-    v[2] = make_float2(b.x, b.y);
-    v[3] = make_float2(b.z, b.w);
-  } else {
-    const double2 *q = reinterpret_cast<const double2 *>(base) + s0;
-#pragma unroll
-    for (int j = 0; j < UQ; ++j) v[j] = q[j];
-  }
-}
+template <typename T, typename C, typename X> struct FlatNode {
+  size_t slot;
+  V2<X> u;
+  V2<T> r, p, ap;
+  C s_ll, s_lh, s_rl, s_rh;
+  unsigned m;
+  bool ok;
+};
 
-// scales of element column c at rows y0-1 .. y0+3 (e0 = the slot of row y0,
-// a multiple of 4), zero for columns outside the grid or when not needed
-template <typename T, typename C, bool NEED>
-__device__ __forceinline__ void ldg_scales5(const T *__restrict__ s, int c, int nx, size_t e0,
-                                            C (&o)[UQ + 1]) {
-  if (!NEED || c < 0 || c >= nx) {
-#pragma unroll
-    for (int j = 0; j <= UQ; ++j) o[j] = C(0);
-    return;
+// loads of grid node n (compact numbering) for the flat kernels; UPD also
+// loads u, p and Ap (the update), otherwise only r
+template <typename T, typename C, typename X, bool SCALES, bool UPD>
+__device__ __forceinline__ void flat_load(FlatNode<T, C, X> &d, int n, int total, int ny1,
+                                          double inv, int nx, int P, const X *__restrict__ u,
+                                          const T *__restrict__ r, const T *__restrict__ p,
+                                          const T *__restrict__ ap, const T *__restrict__ s,
+                                          const uint8_t *__restrict__ mask) {
+  d.ok = n < total;
+  d.s_ll = d.s_lh = d.s_rl = d.s_rh = C(0);
+  if (!d.ok) return;
+  const int c = div_exact(n, ny1, inv), y = n - c * ny1;
+  d.slot = (size_t)c * P + y + LEAD;
+  d.r = ld2<T>(r, d.slot);
+  if constexpr (UPD) {
+    d.u = ld2<X>(u, d.slot);
+    d.p = ld2<T>(p, d.slot);
+    d.ap = ld2<T>(ap, d.slot);
   }
-  o[0] = C(s[e0 - 1]);
-  if constexpr (sizeof(T) == 4) {
-    const float4 a = *reinterpret_cast<const float4 *>(s + e0);
-    o[1] = a.x;
-    o[2] = a.y;
-    o[3] = a.z;
-    o[4] = a.w;
-  } else {
-    const double2 a = *reinterpret_cast<const double2 *>(s + e0);
-    const double2 b = *reinterpret_cast<const double2 *>(s + e0 + 2);
-    o[1] = C(a.x);
-    o[2] = C(a.y);
-    o[3] = C(b.x);
-    o[4] = C(b.y);
+  d.m = mask[d.slot];
+  if constexpr (SCALES) {
+    if (c >= 1) {
+      d.s_ll = C(s[d.slot - P - 1]);
+      d.s_lh = C(s[d.slot - P]);
+    }
+    if (c < nx) {
+      d.s_rl = C(s[d.slot - 1]);
+      d.s_rh = C(s[d.slot]);
+    }
   }
 }
 
@@ -637,56 +489,46 @@ __device__ __forceinline__ void update_flat_run(const UpdArgs &a, int bx, int gx
   const double alpha = ctl->alpha;
   const C alpha_c = C(alpha);
   const T *__restrict__ p = static_cast<const T *>((ctl->it & 1) ? a.pa : a.pb);
-  const int nx = a.nx, ny = a.ny, P = a.P;
-  const int Q = (ny + 1 + UQ - 1) / UQ;  // runs of UQ rows per node column
-  const double invQ = 1.0 / Q;
+  const int nx = a.nx, ny1 = a.ny + 1, P = a.P;
+  const double inv = 1.0 / ny1;
   const T *__restrict__ s = static_cast<const T *>(a.s);
   X *__restrict__ u = static_cast<X *>(a.u);
   T *__restrict__ r = static_cast<T *>(a.r);
   T *__restrict__ zo = static_cast<T *>(a.z);
   const T *__restrict__ ap = static_cast<const T *>(a.ap);
   const uint8_t *__restrict__ mask = a.mask;
-  const int total = (nx + 1) * Q;
+  const int total = (nx + 1) * ny1;
+  const int lane = threadIdx.x & 31;
+  const int warp = (bx * blockDim.x + threadIdx.x) >> 5, nwarps = (gx * blockDim.x) >> 5;
   double acc[2] = {0.0, 0.0};
-  for (int n = bx * blockDim.x + threadIdx.x; n < total; n += gx * blockDim.x) {
-    const int c = div_exact(n, Q, invQ), y0 = UQ * (n - c * Q);
-    const size_t s0 = (size_t)c * P + LEAD + y0;
-    unsigned ok = 0;  // bit j: row y0 + j is a grid row
+  for (int base = warp * RUN; base < total; base += nwarps * RUN) {
+    FlatNode<T, C, X> d[UQ];
 #pragma unroll
     for (int j = 0; j < UQ; ++j)
-      if (y0 + j <= ny) ok |= 1u << j;
-    V2<X> uu[UQ];
-    V2<T> rr[UQ], pp[UQ], aa[UQ];
-    ldg_quad<X>(u, s0, uu);
-    ldg_quad<T>(r, s0, rr);
-    ldg_quad<T>(p, s0, pp);
-    ldg_quad<T>(ap, s0, aa);
-    C sl[UQ + 1], sr[UQ + 1];  // element columns c-1 and c, rows y0-1 .. y0+3
-    ldg_scales5<T, C, PRE != TPO_PRECOND_NONE>(s, c - 1, nx, s0 - P, sl);
-    ldg_scales5<T, C, PRE != TPO_PRECOND_NONE>(s, c, nx, s0, sr);
-    const unsigned mq = *reinterpret_cast<const unsigned *>(mask + s0);
-    V2<X> un[UQ];
-    V2<T> rn[UQ], zt[UQ];
+      flat_load<T, C, X, PRE != TPO_PRECOND_NONE, true>(d[j], base + 32 * j + lane, total, ny1,
+                                                         inv, nx, P, u, r, p, ap, s, mask);
 #pragma unroll
     for (int j = 0; j < UQ; ++j) {
+      if (!d[j].ok) continue;
       // the solution accumulates in FP64 in every form
-      un[j] = mk2<X>(X(fma(alpha, (double)pp[j].x, (double)uu[j].x)),
-                     X(fma(alpha, (double)pp[j].y, (double)uu[j].y)));
-      rn[j] = mk2<T>(T(fmaT(-alpha_c, C(aa[j].x), C(rr[j].x))),
-                     T(fmaT(-alpha_c, C(aa[j].y), C(rr[j].y))));
+      const V2<X> un = mk2<X>(X(fma(alpha, (double)d[j].p.x, (double)d[j].u.x)),
+                              X(fma(alpha, (double)d[j].p.y, (double)d[j].u.y)));
+      const V2<T> rn = mk2<T>(T(fmaT(-alpha_c, C(d[j].ap.x), C(d[j].r.x))),
+                              T(fmaT(-alpha_c, C(d[j].ap.y), C(d[j].r.y))));
+      st2<X>(u, d[j].slot, un);
+      st2<T>(r, d[j].slot, rn);
       C pa, pb, pd;
-      node_pre<C, PRE>((mq >> (8 * j)) & 0xffu, sl[j], sl[j + 1], sr[j], sr[j + 1], pa, pb, pd);
-      const V2<C> z = pre_apply<C>(pa, pb, pd, cvt2<C, T>(rn[j]));
-      zt[j] = mk2<T>(T(z.x), T(z.y));
-      if ((ok >> j) & 1u) {
-        // r.z with the stored (rounded) z, the one the direction update uses
-        acc[0] += zo ? dot2d(rn[j], zt[j]) : dot2d(rn[j], z);
-        acc[1] += dot2d(rn[j], rn[j]);
+      node_pre<C, PRE>(d[j].m, d[j].s_ll, d[j].s_lh, d[j].s_rl, d[j].s_rh, pa, pb, pd);
+      const V2<C> z = pre_apply<C>(pa, pb, pd, cvt2<C, T>(rn));
+      if (zo) {  // r.z with the stored (rounded) z, the one the direction update uses
+        const V2<T> zt = mk2<T>(T(z.x), T(z.y));
+        st2<T>(zo, d[j].slot, zt);
+        acc[0] += dot2d(rn, zt);
+      } else {
+        acc[0] += dot2d(rn, z);
       }
+      acc[1] += dot2d(rn, rn);
     }
-    stg_pairs<X>(u, s0, un, ok);
-    stg_pairs<T>(r, s0, rn, ok);
-    if (zo) stg_pairs<T>(zo, s0, zt, ok);
   }
   if (!grid_reduce<2>(acc, a.part, &ctl->counter, nb, bid)) return;
   if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
@@ -699,30 +541,26 @@ __device__ __forceinline__ void precond_flat_run(int nx, int ny, int P, const T 
                                                  const uint8_t *__restrict__ mask,
                                                  const T *__restrict__ r, T *__restrict__ z,
                                                  int bx, int gx) {
-  const int Q = (ny + 1 + UQ - 1) / UQ;
-  const double invQ = 1.0 / Q;
-  const int total = (nx + 1) * Q;
-  for (int n = bx * blockDim.x + threadIdx.x; n < total; n += gx * blockDim.x) {
-    const int c = div_exact(n, Q, invQ), y0 = UQ * (n - c * Q);
-    const size_t s0 = (size_t)c * P + LEAD + y0;
-    unsigned ok = 0;
+  const int ny1 = ny + 1;
+  const double inv = 1.0 / ny1;
+  const int total = (nx + 1) * ny1;
+  const int lane = threadIdx.x & 31;
+  const int warp = (bx * blockDim.x + threadIdx.x) >> 5, nwarps = (gx * blockDim.x) >> 5;
+  for (int base = warp * RUN; base < total; base += nwarps * RUN) {
+    FlatNode<T, C, T> d[UQ];
 #pragma unroll
     for (int j = 0; j < UQ; ++j)
-      if (y0 + j <= ny) ok |= 1u << j;
-    V2<T> rr[UQ], zt[UQ];
-    ldg_quad<T>(r, s0, rr);
-    C sl[UQ + 1], sr[UQ + 1];
-    ldg_scales5<T, C, PRE != TPO_PRECOND_NONE>(s, c - 1, nx, s0 - P, sl);
-    ldg_scales5<T, C, PRE != TPO_PRECOND_NONE>(s, c, nx, s0, sr);
-    const unsigned mq = *reinterpret_cast<const unsigned *>(mask + s0);
+      flat_load<T, C, T, PRE != TPO_PRECOND_NONE, false>(d[j], base + 32 * j + lane, total, ny1,
+                                                          inv, nx, P, nullptr, r, nullptr,
+                                                          nullptr, s, mask);
 #pragma unroll
     for (int j = 0; j < UQ; ++j) {
+      if (!d[j].ok) continue;
       C pa, pb, pd;
-      node_pre<C, PRE>((mq >> (8 * j)) & 0xffu, sl[j], sl[j + 1], sr[j], sr[j + 1], pa, pb, pd);
-      const V2<C> zz = pre_apply<C>(pa, pb, pd, cvt2<C, T>(rr[j]));
-      zt[j] = mk2<T>(T(zz.x), T(zz.y));
+      node_pre<C, PRE>(d[j].m, d[j].s_ll, d[j].s_lh, d[j].s_rl, d[j].s_rh, pa, pb, pd);
+      const V2<C> zz = pre_apply<C>(pa, pb, pd, cvt2<C, T>(d[j].r));
+      st2<T>(z, d[j].slot, mk2<T>(T(zz.x), T(zz.y)));
     }
-    stg_pairs<T>(z, s0, zt, ok);
   }
 }
 template <typename T, typename C, int PRE>

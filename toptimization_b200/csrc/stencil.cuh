@@ -70,29 +70,6 @@ __device__ __forceinline__ void elem_forces(T s, V2<T> bl, V2<T> br, V2<T> tr, V
   ftl = mk2<T>(-(PmQ + hx), RmQ - hy);
 }
 
-// elem_forces on x/y pairs: the same operations in the same order, issued as
-// two-wide arithmetic (packed FP32 instructions when T is float).
-template <typename T>
-__device__ __forceinline__ void elem_forces2(T s, V2<T> bl, V2<T> br, V2<T> tr, V2<T> tl,
-                                             V2<T> &fbl, V2<T> &fbr, V2<T> &ftr, V2<T> &ftl) {
-  const V2<T> A = sub2(tr, bl);  // (a, ay)
-  const V2<T> B = sub2(br, tl);  // (b, by)
-  const V2<T> S = add2(A, B);    // (a + b, ay + by)
-  const V2<T> D = sub2(A, B);    // (a - b, ay - by)
-  const T apb = S.x, ayb = D.y;
-  const V2<T> PR = mul2(bc2<T>(s), fma2(mk2<T>(kst<T>(0), kst<T>(1)), bc2<T>(apb),
-                                        mul2(mk2<T>(kst<T>(1), kst<T>(0)), bc2<T>(ayb))));
-  const T Q = s * kst<T>(2) * (D.x + S.y);
-  const V2<T> H = mul2(bc2<T>(s * kst<T>(3)), sub2(add2(bl, tr), add2(br, tl)));  // (hx, hy)
-  const V2<T> PQ = add2(PR, bc2<T>(Q));   // (P + Q, R + Q)
-  const V2<T> PmQ = sub2(PR, bc2<T>(Q));  // (P - Q, R - Q)
-  const V2<T> nH = mk2<T>(-H.x, -H.y);
-  fbl = sub2(H, PQ);
-  fbr = fma2(PmQ, mk2<T>(T(1), T(-1)), nH);
-  ftr = add2(PQ, H);
-  ftl = fma2(PmQ, mk2<T>(T(-1), T(1)), nH);
-}
-
 // Point preconditioners computed on the fly from the node's four element
 // scales (same argument order as node_apply).
 //  JACOBI: z = r / diag, diag_i = sum_e s_e Ke_ii, fixed -> 1, floor 1e-20
