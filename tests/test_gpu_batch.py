@@ -69,6 +69,33 @@ def test_batch_matches_single_design_solver(tpo_built):
         assert abs(rho.mean() - pr.volfrac) < 1e-3
 
 
+def test_batch_matches_oracle(tpo_built):
+    """Batched (mixed-form) designs against the FP64 oracle's own run of the
+    same problems (oracle/simp64.py, the reference's loop
+    src/toptimization/optimizer/simp.py:141-219): the first OC iteration
+    (same input density) to the PCG tolerance, the 5-iteration compliance and
+    volume histories and the final density to the OC-bisection scale (its
+    multiplier is a discrete function of dc)."""
+    from oracle import simp64 as O
+    ps = _designs(3, seed=17, lo=64, hi=110, iters=5)
+    res = _run(ps)
+    for i, pr in enumerate(ps):
+        ref = O.run(pr)
+        rho, h = res[i]
+        cb = np.asarray(h["compliance"])
+        assert len(cb) == len(ref.compliance) == pr.max_iter
+        e_first = abs(cb[0] - ref.compliance[0]) / ref.compliance[0]
+        e_all = float(np.max(np.abs(cb - ref.compliance) / ref.compliance))
+        e_rho = float(np.abs(np.asarray(rho).reshape(-1) - ref.rho).max())
+        e_vol = float(np.abs(np.asarray(h["volume"]) - ref.volume).max())
+        print(f"design {i} ({pr.nelx}x{pr.nely}): compliance first {e_first:.2e}, "
+              f"worst {e_all:.2e}; density max-abs {e_rho:.2e}; volume {e_vol:.2e}")
+        assert e_first < 1e-7
+        assert e_all < 1e-4
+        assert e_vol < 1e-4
+        assert e_rho < 1e-2
+
+
 def test_slots_release_and_stop_rule(tpo_built):
     ps = _designs(3, seed=13, iters=4)
     b = Batch(2)

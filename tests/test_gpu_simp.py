@@ -3,11 +3,13 @@
 FP64 (tests/golden/ref_run_*.npz) and against the oracles.
 
 Tolerances: compliance history 1e-9 relative (every iteration); density
-max-abs 5e-8 after 100 OC iterations. Two FP64 CPU implementations of the
-same algorithm (the reference's own code and oracle/simp64.py) already differ
-by 1.7e-8 in density there: single CG stop points move by one iteration and
-the OC dynamics amplify rounding (the spread is still 5e-9 after 60
-iterations at cg_tol 1e-12).
+max-abs 2.5e-8 after 100 OC iterations of the MBB 60x20 (measured on B200:
+1.65e-8). Two FP64 CPU implementations of the same algorithm (the reference's
+own code and oracle/simp64.py) already differ by 1.7e-8 in density there:
+single CG stop points move by one iteration and the OC dynamics amplify
+rounding; the bound is that spread with a margin of 1.5. At cg_tol 1e-12
+(no stop point moves) the GPU is within 3.9e-9 (bound 1e-8); on the shorter
+runs (12-53 OC iterations) within 4e-9 (bounds 5e-9 and 1e-8).
 """
 
 import copy
@@ -52,7 +54,7 @@ def test_mbb_60x20_100_iterations_vs_reference(tpo_built):
     assert e["n"] == e["n_ref"] == 100
     assert e["comp"] < 1e-9
     assert e["vol"] < 1e-9
-    assert e["rho"] < 5e-8
+    assert e["rho"] < 2.5e-8
     # stop points move where the residual crawls along the threshold
     assert e["cg"] <= 10
 
@@ -64,7 +66,7 @@ def test_mbb_60x20_tight_tolerance_vs_reference(tpo_built):
     rho, hist = gpu_run(pr)
     e = errors(rho, hist, g)
     print("mbb_60x20 cg_tol 1e-12 vs reference:", e)
-    assert e["comp"] < 1e-10 and e["rho"] < 2e-8 and e["cg"] <= 1
+    assert e["comp"] < 1e-10 and e["rho"] < 1e-8 and e["cg"] <= 1
 
 
 @pytest.mark.parametrize("name,ov", [
@@ -101,7 +103,7 @@ def test_bridge_100x50_vs_reference(tpo_built):
     rho, hist = gpu_run(bridge_100x50())
     e = errors(rho, hist, g)
     print("bridge_100x50", e)
-    assert e["comp"] < 1e-9 and e["rho"] < 5e-8 and e["cg"] <= 2
+    assert e["comp"] < 1e-9 and e["rho"] < 1e-8 and e["cg"] <= 2
 
 
 def test_nodal_block_jacobi_vs_oracle(tpo_built):

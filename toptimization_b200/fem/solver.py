@@ -60,7 +60,7 @@ class PCGSolver:
     def __init__(self, nelx: int, nely: int, e_min: float, penalty: float,
                  f_norm_sq: float, *, preconditioner: str = "jacobi",
                  precision: str = "fp64", max_iter: int = 2000, tol: float = 1e-8,
-                 inner_tol: float = 1e-4, max_outer: int = 50, poll_every: int = 0,
+                 inner_tol: float = 1e-3, max_outer: int = 50, poll_every: int = 0,
                  recurrence: str = "auto", device=None, nelz: int = 0):
         if preconditioner not in _lib.PRECOND:
             raise ValueError(f"unknown preconditioner {preconditioner!r}")

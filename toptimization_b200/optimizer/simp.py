@@ -119,7 +119,7 @@ class SimpDesign:
         self.solver = PCGSolver(pr.nelx, pr.nely, pr.E_min, pr.penalty, self.f_norm_sq,
                                 preconditioner=self.preconditioner, precision=self.precision,
                                 max_iter=pr.max_cg_iter, tol=pr.cg_tol,
-                                inner_tol=getattr(pr, "inner_tol", 1e-4),
+                                inner_tol=getattr(pr, "inner_tol", 1e-3),
                                 max_outer=getattr(pr, "max_outer_iter", 50),
                                 recurrence=getattr(pr, "recurrence", "auto"),
                                 poll_every=poll_every, device=dev, nelz=nelz)
