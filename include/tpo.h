@@ -50,7 +50,10 @@ enum {
   TPO_SOLVE_MAX_ITER = 2,
   TPO_SOLVE_BREAKDOWN = 3,   /* |p.Ap| < 1e-30 (reference solver.py:114-115) */
   TPO_SOLVE_NONFINITE = 4,
-  TPO_SOLVE_ZERO_RHS = 5     /* ||f|| < 1e-30: u = 0 (reference solver.py:61-63) */
+  TPO_SOLVE_ZERO_RHS = 5,    /* ||f|| < 1e-30: u = 0 (reference solver.py:61-63) */
+  TPO_SOLVE_TIMEOUT = 7,     /* tpo_pcg_solve_async: a bounded pipeline wait ran out */
+  TPO_SOLVE_LOOP_LIMIT = 8   /* tpo_pcg_solve_async: the device loop reached its body
+                                limit with the solve still running */
 };
 
 /* Preconditioners. */
@@ -153,6 +156,25 @@ int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c,
                   const double *rho_phys, const double *f, const uint8_t *fixed,
                   double *u, void *ws, size_t ws_bytes,
                   tpo_solve_result *out, tpo_stream s);
+
+/* The same solve, asynchronous on the stream (replaces the host loop of the
+ * reference's fem/solver.py:107-156): no host synchronisation; the PCG loop
+ * runs on the device as a CUDA graph conditional WHILE node (bodies of 16
+ * iterations, the stop, breakdown and refinement rules decided by the
+ * kernels, a bound on the number of bodies), and the result is written to
+ * `out_dev`, DEVICE memory (8-byte aligned), when the solve has finished.
+ * Same kernels in the same order as tpo_pcg_solve, so the same results.
+ * If `s` is capturing, the solve's nodes are added to that capture (so a
+ * whole OC iteration can be one graph); otherwise the call captures them
+ * itself and launches the graph once. Make one call (or tpo_pcg_solve) on a
+ * device before capturing: launch plans are set up on first use. ws, u and
+ * out_dev must stay valid until the stream reaches the end of the solve.
+ * Errors found while enqueueing are returned; a pipeline wait that runs out
+ * shows as TPO_SOLVE_TIMEOUT in out_dev->status. */
+int tpo_pcg_solve_async(const tpo_grid *g, const tpo_solve_cfg *c,
+                        const double *rho_phys, const double *f, const uint8_t *fixed,
+                        double *u, void *ws, size_t ws_bytes,
+                        tpo_solve_result *out_dev, tpo_stream s);
 
 /* ---- compliance and sensitivity --------------------------------------------
  * dc[e] = -p rho^(p-1) (1-e_min) u_e^T Ke u_e; *compliance_out (device) =

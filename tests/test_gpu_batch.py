@@ -182,14 +182,15 @@ def test_admission_respects_the_memory_budget(tpo_built):
     assert rep.peak_resident <= 2 and rep.peak_bytes <= budget
 
 
-def test_graph_engine_run_matches_direct(tpo_built):
-    """simp.run(engine="graph"): each OC iteration one CUDA graph launch,
-    same OC rules; first-iteration compliance equal to the direct mixed run to
-    the PCG tolerance, the history to the bisection scale."""
+def test_batch_engine_run_matches_direct(tpo_built):
+    """simp.run(engine="batch"): the design through the batched engine, each
+    OC iteration one CUDA graph launch, same OC rules; first-iteration
+    compliance equal to the direct mixed run to the PCG tolerance, the history
+    to the bisection scale."""
     from toptimization_b200.optimizer.simp import RunHistory, run
     pr = _designs(1, seed=17, lo=80, hi=120, iters=6)[0]
     hg, hd = RunHistory(), RunHistory()
-    rg = run(pr, verbose=False, save=False, history=hg, engine="graph")
+    rg = run(pr, verbose=False, save=False, history=hg, engine="batch")
     rd = run(pr, verbose=False, save=False, history=hd, precision="mixed")
     assert rg.shape == rd.shape == (pr.nelx, pr.nely)
     cg, cd = np.array(hg.compliance), np.array(hd.compliance)

@@ -17,7 +17,7 @@ LIB_PATH = Path(os.environ.get("TPO_LIBRARY", Path(__file__).with_name("libtpo.s
 
 TPO_OK = 0
 SOLVE_STATUS = {0: "running", 1: "converged", 2: "max_iter", 3: "breakdown",
-                4: "nonfinite", 5: "zero_rhs"}
+                4: "nonfinite", 5: "zero_rhs", 7: "timeout", 8: "loop_limit"}
 PRECOND = {"none": 0, "jacobi": 1, "block_jacobi": 2, "nodal_block_jacobi": 3}
 PRECISION = {"fp64": 0, "mixed": 1}
 
@@ -98,6 +98,9 @@ _SIGS = {
     "tpo_pcg_solve": (c_int, [POINTER(TpoGrid), POINTER(TpoSolveCfg), c_void_p, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_size_t, POINTER(TpoSolveResult),
                               c_void_p]),
+    "tpo_pcg_solve_async": (c_int, [POINTER(TpoGrid), POINTER(TpoSolveCfg), c_void_p,
+                                    c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
+                                    c_void_p]),
     "tpo_sensitivity_workspace_bytes": (c_size_t, [POINTER(TpoGrid)]),
     "tpo_sensitivity": (c_int, [POINTER(TpoGrid), c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_size_t, c_void_p]),

@@ -306,6 +306,7 @@ struct PcgWs {
   float *fra, *frb, *fpa, *fpb, *fap, *fz;       // mixed: FP32 Krylov vectors (u stays FP64)
   double *wa, *wb, *sa, *sb;                   // one-launch form: w = K M^-1 r, s = K p
   bool single;                                 // one launch per iteration (k_cgstep)
+  uint32_t *bodies;                            // asynchronous solve: loop bodies run
   int P;
   size_t bytes;
 };
@@ -327,6 +328,7 @@ PcgWs carve_pcg(void *base, const tpo_grid *g, const tpo_solve_cfg *c) {
   w.P = P;
   w.ctl = cv.take<PcgCtl>(1);
   w.octl = cv.take<OuterCtl>(1);
+  w.bodies = cv.take<uint32_t>(1);
   w.part = cv.take<double>(3 * (size_t)max_ctas(g));  // up to 3 sums per CTA
   w.mask = cv.take<uint8_t>(NN);
   w.u = cv.take<double>(2 * NN);
@@ -914,6 +916,273 @@ int pcg_single(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, con
   return TPO_OK;
 }
 
+// ----------------------------------------------------------------- asynchronous PCG
+// tpo_pcg_solve_async: the same solve as tpo_pcg_solve, enqueued on the stream
+// with no host synchronisation. The PCG loop is a CUDA graph conditional
+// WHILE node whose body holds kAsyncBody iterations; after each body one
+// thread decides on the device whether another is needed (the stop rules are
+// the kernels' own; a body limit bounds the loop). A last kernel writes the
+// tpo_solve_result into device memory.
+constexpr int kAsyncBody = 16;
+
+__global__ void k_solve_cond(const PcgCtl *ctl, const OuterCtl *octl, uint32_t *bodies,
+                             uint32_t max_bodies, cudaGraphConditionalHandle h) {
+  bool more;
+  if (octl)  // mixed: the outer solve runs; the inner one runs or awaits a replacement
+    more = octl->status == TPO_SOLVE_RUNNING &&
+           (ctl->status == TPO_SOLVE_RUNNING || ctl->status == SOLVE_NEED_UPDATE);
+  else
+    more = ctl->status == TPO_SOLVE_RUNNING;
+  if (ctl->err) more = false;
+  const uint32_t b = ++*bodies;
+  if (b >= max_bodies) more = false;
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+// The host epilogues of pcg_fp64 / pcg_single / pcg_mixed, on the device.
+__global__ void k_solve_result(const PcgCtl *ctl, const OuterCtl *octl, const uint32_t *bodies,
+                               uint32_t max_bodies, int max_iter, tpo_solve_result *out) {
+  int status;
+  tpo_solve_result r{};
+  if (octl) {
+    if (octl->status != TPO_SOLVE_RUNNING) status = octl->status;
+    else if (ctl->status != TPO_SOLVE_RUNNING && ctl->status != SOLVE_NEED_UPDATE)
+      status = ctl->status;  // the inner solve stopped (max_iter, breakdown, non-finite)
+    else
+      status = TPO_SOLVE_MAX_ITER;
+    r.iters = ctl->it;
+    r.updates = ctl->it;
+    r.outer_iters = octl->it;
+    r.rr = octl->rr;
+  } else {
+    status = ctl->status;
+    if (status == TPO_SOLVE_RUNNING) status = TPO_SOLVE_MAX_ITER;
+    r.updates = ctl->it;
+    r.iters = status == TPO_SOLVE_CONVERGED ? ctl->it : max_iter;
+    r.outer_iters = 1;
+    r.rr = ctl->rr;
+  }
+  if (ctl->err) status = TPO_SOLVE_TIMEOUT;
+  else if (*bodies >= max_bodies && (status == TPO_SOLVE_MAX_ITER) &&
+           (octl ? octl->status == TPO_SOLVE_RUNNING : ctl->status == TPO_SOLVE_RUNNING))
+    status = TPO_SOLVE_LOOP_LIMIT;
+  r.status = status;
+  *out = r;
+}
+
+__global__ void k_solve_zero_rhs(tpo_solve_result *out) {
+  tpo_solve_result r{};
+  r.status = TPO_SOLVE_ZERO_RHS;
+  r.outer_iters = 1;
+  *out = r;
+}
+
+// two private non-blocking streams per device: one into which the loop body
+// is captured, one into which a solve is captured when the caller's stream is
+// not capturing (the caller's stream may be the legacy default stream, which
+// cannot be captured; the finished graph is launched on it instead)
+cudaStream_t g_body_stream[kMaxDevices], g_cap_stream[kMaxDevices];
+std::mutex g_body_mu;
+int capture_streams(cudaStream_t *body, cudaStream_t *cap) {
+  int dev;
+  int rc = current_device(&dev);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_body_mu);
+  if (!g_body_stream[dev])
+    TPO_CK(cudaStreamCreateWithFlags(&g_body_stream[dev], cudaStreamNonBlocking));
+  if (!g_cap_stream[dev])
+    TPO_CK(cudaStreamCreateWithFlags(&g_cap_stream[dev], cudaStreamNonBlocking));
+  if (body) *body = g_body_stream[dev];
+  if (cap) *cap = g_cap_stream[dev];
+  return TPO_OK;
+}
+
+// Inserts the loop into the capture that `st` is running: a WHILE node after
+// the work captured so far, its body captured from `emit(body_stream)`, and
+// the stream's later work ordered after the node.
+template <typename BodyFn>
+int add_while_loop(cudaStream_t st, BodyFn emit, const PcgCtl *ctl, const OuterCtl *octl,
+                   uint32_t *bodies, uint32_t max_bodies) {
+  cudaStreamCaptureStatus cst;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  TPO_CK(cudaStreamGetCaptureInfo(st, &cst, nullptr, &g, &deps, &ndeps));
+  if (cst != cudaStreamCaptureStatusActive || !g)
+    return fail(TPO_ERR_CUDA, "the stream is not capturing");
+  std::vector<cudaGraphNode_t> pre(deps, deps + ndeps);
+  cudaGraphConditionalHandle h;
+  TPO_CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  TPO_CK(cudaGraphAddNode(&cnode, g, pre.data(), pre.size(), &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaStream_t bs;
+  int rc = capture_streams(&bs, nullptr);
+  if (rc) return rc;
+  TPO_CK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeRelaxed));
+  rc = emit(bs);
+  if (!rc) {
+    k_solve_cond<<<1, 1, 0, bs>>>(ctl, octl, bodies, max_bodies, h);
+    if (cudaPeekAtLastError() != cudaSuccess) rc = fail(TPO_ERR_CUDA, "loop condition launch");
+  }
+  cudaGraph_t tmp;
+  const cudaError_t e = cudaStreamEndCapture(bs, &tmp);
+  if (rc) return rc;
+  TPO_CK(e);
+  TPO_CK(cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies));
+  return TPO_OK;
+}
+
+// The whole solve of one form enqueued on `st`, which is capturing: the
+// set-up of pcg_mixed / pcg_single / pcg_fp64, the loop, the epilogue. Same
+// kernels in the same order as the host-driven solve, so the same results.
+template <int PRE>
+int emit_solve_async(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho,
+                     const double *f, const uint8_t *fixed, double *u, const PcgWs &w,
+                     tpo_solve_result *out, cudaStream_t st, double alpha_reg) {
+  const int nx = g->nelx, ny = g->nely, P = w.P;
+  const size_t NN = (size_t)(nx + 1) * P;
+  constexpr bool block = PRE == TPO_PRECOND_BLOCK_JACOBI;
+  const bool mixed = c->precision == TPO_PRECISION_MIXED;
+  const double fn = std::sqrt(c->f_norm_sq);
+  const double tol_sq = (c->tol * fn) * (c->tol * fn);
+  const dim3 sg = flat_grid((size_t)nx * P, 256, sm_count() * 16);
+  int rc = pack_inputs(g, w, f, fixed, u, c->warm_start != 0, st);
+  if (rc) return rc;
+  if ((rc = zero_vectors(w, NN, st))) return rc;
+  TPO_CK(cudaMemsetAsync(w.bodies, 0, sizeof(uint32_t), st));
+  constexpr int m = kAsyncBody;
+  uint32_t max_bodies = 0;
+  if (mixed) {
+    k_scales<<<sg, 256, 0, st>>>(nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, w.s32,
+                                 nullptr, block ? w.w32 : nullptr);
+    TPO_CK_LAUNCH();
+    const double delta = c->inner_tol > 0.0 ? c->inner_tol : 1e-3;
+    k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, delta * delta, c->max_iter, w.octl, tol_sq,
+                                c->max_outer);
+    TPO_CK_LAUNCH();
+    TsArgs rx{};
+    rx.nx = nx; rx.ny = ny; rx.P = P;
+    rx.s = w.s64; rx.mask = w.mask; rx.a = w.u; rx.uw = w.u; rx.f = w.f;
+    rx.out = w.fra; rx.out2 = block ? w.frb : nullptr;  // block: by iteration parity
+    rx.part = w.part; rx.ctl = w.ctl; rx.octl = w.octl; rx.err = &w.ctl->err;
+    BlkArgs b{};
+    b.nx = nx; b.ny = ny; b.P = P;
+    b.w = w.w32; b.mask = w.mask; b.u = w.u; b.ap = w.fap; b.pa = w.fpa; b.pb = w.fpb;
+    b.ra = w.fra; b.rb = w.frb; b.z = w.fz; b.part = w.part; b.ctl = w.ctl;
+    TsArgs d{};
+    d.nx = nx; d.ny = ny; d.P = P;
+    d.s = w.s32; d.mask = w.mask; d.a = w.fz; d.pa = w.fpa; d.pb = w.fpb; d.out = w.fap;
+    d.part = w.part; d.ctl = w.ctl; d.err = &w.ctl->err;
+    UpdArgs up{};
+    up.nx = nx; up.ny = ny; up.P = P;
+    up.s = w.s32; up.mask = w.mask; up.u = w.u; up.r = w.fra; up.ap = w.fap; up.pa = w.fpa;
+    up.pb = w.fpb; up.part = w.part; up.ctl = w.ctl; up.z = w.fz;
+    // a body: the FP64 residual replacement (a no-op unless one is due), z of
+    // a replaced residual, then m inner iterations (no-ops once one is due)
+    max_bodies = (uint32_t)((c->max_iter + m - 1) / m + c->max_outer + 2);
+    auto body = [&](cudaStream_t bs) -> int {
+      StencilCfg<double, double, M_RESX, PRE>::launch(bs, rx, nx, ny);
+      TPO_CK_LAUNCH();
+      if (block) {
+        BlkArgs bi = b;
+        bi.gate = 1;
+        k_blockpre<float, double, true, kBlkL, double><<<blk_grid(nx, ny), ST_THREADS, 0, bs>>>(bi);
+      } else {
+        k_precond_gated<float, double, PRE>
+            <<<flat_wave<k_precond_gated<float, double, PRE>>(nx, ny), UF_THREADS, 0, bs>>>(
+                w.ctl, nx, ny, P, w.s32, w.mask, w.fra, w.fz);
+      }
+      TPO_CK_LAUNCH();
+      for (int i = 0; i < m; ++i) {
+        StencilCfg<float, double, M_DIR, TPO_PRECOND_BLOCK_JACOBI>::launch(bs, d, nx, ny);
+        TPO_CK_LAUNCH();
+        if (block)
+          k_blockpre<float, double, false, kBlkL, double><<<blk_grid(nx, ny), ST_THREADS, 0, bs>>>(b);
+        else
+          k_update_flat<float, double, PRE, double>
+              <<<flat_wave<k_update_flat<float, double, PRE, double>>(nx, ny), UF_THREADS, 0, bs>>>(up);
+        TPO_CK_LAUNCH();
+      }
+      return TPO_OK;
+    };
+    rc = add_while_loop(st, body, w.ctl, w.octl, w.bodies, max_bodies);
+  } else {
+    k_scales<<<sg, 256, 0, st>>>(nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, nullptr,
+                                 block ? w.w64 : nullptr, nullptr);
+    TPO_CK_LAUNCH();
+    k_ctl_init<<<1, 1, 0, st>>>(w.ctl, tol_sq, 0.0, c->max_iter, nullptr, 0.0, 0);
+    TPO_CK_LAUNCH();
+    TsArgs a{};
+    a.nx = nx; a.ny = ny; a.P = P;
+    a.s = w.s64; a.mask = w.mask; a.a = w.u; a.uw = w.u; a.f = w.f; a.out = w.ra;
+    a.part = w.part; a.ctl = w.ctl; a.err = &w.ctl->err;
+    StencilCfg<double, double, M_RES, PRE>::launch(st, a, nx, ny);
+    TPO_CK_LAUNCH();
+    if (w.single) {
+      const CgArgs ca = cg_args(g, w);
+      // the first launch of the first body is the INIT launch
+      max_bodies = (uint32_t)((c->max_iter + 1 + m - 1) / m + 2);
+      auto body = [&](cudaStream_t bs) -> int {
+        for (int i = 0; i < m; ++i) {
+          CgCfg<double, double, PRE>::launch(bs, ca, nx, ny);
+          TPO_CK_LAUNCH();
+        }
+        return TPO_OK;
+      };
+      rc = add_while_loop(st, body, w.ctl, nullptr, w.bodies, max_bodies);
+    } else {
+      BlkArgs b{};
+      b.nx = nx; b.ny = ny; b.P = P;
+      b.w = w.w64; b.mask = w.mask; b.u = w.u; b.ap = w.ap; b.pa = w.pa; b.pb = w.pb;
+      b.ra = w.ra; b.rb = w.rb; b.z = w.z; b.part = w.part; b.ctl = w.ctl;
+      if (block) {
+        k_blockpre<double, double, true, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, st>>>(b);
+      } else {
+        k_precond_flat<double, double, PRE>
+            <<<flat_wave<k_precond_flat<double, double, PRE>>(nx, ny), UF_THREADS, 0, st>>>(
+                nx, ny, P, w.s64, w.mask, w.ra, w.z);
+      }
+      TPO_CK_LAUNCH();
+      TsArgs d{};
+      d.nx = nx; d.ny = ny; d.P = P;
+      d.s = w.s64; d.mask = w.mask; d.a = w.z; d.pa = w.pa; d.pb = w.pb; d.out = w.ap;
+      d.part = w.part; d.ctl = w.ctl; d.err = &w.ctl->err;
+      UpdArgs up{};
+      up.nx = nx; up.ny = ny; up.P = P;
+      up.s = w.s64; up.mask = w.mask; up.u = w.u; up.r = w.ra; up.ap = w.ap; up.pa = w.pa;
+      up.pb = w.pb; up.part = w.part; up.ctl = w.ctl; up.z = w.z;
+      max_bodies = (uint32_t)((c->max_iter + m - 1) / m + 2);
+      auto body = [&](cudaStream_t bs) -> int {
+        for (int i = 0; i < m; ++i) {
+          StencilCfg<double, double, M_DIR, TPO_PRECOND_BLOCK_JACOBI>::launch(bs, d, nx, ny);
+          TPO_CK_LAUNCH();
+          if (block)
+            k_blockpre<double, double, false, kBlkL><<<blk_grid(nx, ny), ST_THREADS, 0, bs>>>(b);
+          else
+            k_update_flat<double, double, PRE>
+                <<<flat_wave<k_update_flat<double, double, PRE>>(nx, ny), UF_THREADS, 0, bs>>>(up);
+          TPO_CK_LAUNCH();
+        }
+        return TPO_OK;
+      };
+      rc = add_while_loop(st, body, w.ctl, nullptr, w.bodies, max_bodies);
+    }
+  }
+  if (rc) return rc;
+  if ((rc = unpack_solution(g, w, u, st))) return rc;
+  k_solve_result<<<1, 1, 0, st>>>(w.ctl, mixed ? w.octl : nullptr, w.bodies, max_bodies,
+                                  c->max_iter, out);
+  TPO_CK_LAUNCH();
+  return TPO_OK;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ matvec (packing)
@@ -1014,7 +1283,8 @@ int tpo_set_stiffness(const double ke[64], const double ke_inv[64], double alpha
   TPO_CK(cudaMemcpyToSymbol(c_kinv_f, kif, sizeof(float) * 64));
   g_alpha_reg[dev] = alpha_reg;
   g_have_stiffness[dev] = true;
-  return TPO_OK;
+  // the asynchronous solve's capture streams, made here, outside any capture
+  return capture_streams(nullptr, nullptr);
 }
 
 // ------------------------------------------------------------------ matvec
@@ -1081,14 +1351,17 @@ size_t tpo_pcg_workspace_bytes(const tpo_grid *g, const tpo_solve_cfg *c) {
   return carve_pcg(nullptr, g, c).bytes;
 }
 
-int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_phys,
-                  const double *f, const uint8_t *fixed, double *u, void *ws, size_t ws_bytes,
-                  tpo_solve_result *out, tpo_stream s) {
+}  // extern "C"
+
+namespace {
+// argument checks shared by tpo_pcg_solve and tpo_pcg_solve_async
+int check_solve_args(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_phys,
+                     const double *f, const uint8_t *fixed, double *u, void *ws,
+                     size_t ws_bytes, const void *out, int *dev) {
   int rc = check_grid(g);
   if (rc) return rc;
   if (!c || !out) return fail(TPO_ERR_ARGS, "cfg and result must be non-NULL");
-  int dev;
-  if ((rc = need_stiffness(&dev))) return rc;
+  if ((rc = need_stiffness(dev))) return rc;
   if (!rho_phys || !f || !fixed || !u || !ws) return fail(TPO_ERR_ARGS, "NULL pointer argument");
   if (!aligned(f, 16) || !aligned(u, 16) || !aligned(ws, kAlign))
     return fail(TPO_ERR_ARGS, "misaligned pointer (nodal vectors need 16 B, workspace 256 B)");
@@ -1107,6 +1380,19 @@ int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_p
     return fail(TPO_ERR_ARGS, "tol and f_norm_sq must be >= 0");
   const PcgWs w = carve_pcg(ws, g, c);
   if (ws_bytes < w.bytes) return fail(TPO_ERR_WORKSPACE, "workspace %zu < %zu", ws_bytes, w.bytes);
+  return TPO_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_phys,
+                  const double *f, const uint8_t *fixed, double *u, void *ws, size_t ws_bytes,
+                  tpo_solve_result *out, tpo_stream s) {
+  int dev;
+  int rc = check_solve_args(g, c, rho_phys, f, fixed, u, ws, ws_bytes, out, &dev);
+  if (rc) return rc;
+  const PcgWs w = carve_pcg(ws, g, c);
   cudaStream_t st = static_cast<cudaStream_t>(s);
   memset(out, 0, sizeof(*out));
 
@@ -1146,6 +1432,67 @@ int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_p
                  ? pcg_mixed<TPO_PRECOND_NODAL_BLOCK>(g, c, rho_phys, f, fixed, u, w, out, st, ar)
                  : pcg_fp64<TPO_PRECOND_NODAL_BLOCK>(g, c, rho_phys, f, fixed, u, w, out, st, ar);
   }
+}
+
+int tpo_pcg_solve_async(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_phys,
+                        const double *f, const uint8_t *fixed, double *u, void *ws,
+                        size_t ws_bytes, tpo_solve_result *out_dev, tpo_stream s) {
+  int dev;
+  int rc = check_solve_args(g, c, rho_phys, f, fixed, u, ws, ws_bytes, out_dev, &dev);
+  if (rc) return rc;
+  if (!aligned(out_dev, 8)) return fail(TPO_ERR_ARGS, "misaligned result pointer (8 B)");
+  const PcgWs w = carve_pcg(ws, g, c);
+  const cudaStream_t user = static_cast<cudaStream_t>(s);
+  cudaStreamCaptureStatus cs;
+  TPO_CK(cudaStreamIsCapturing(user, &cs));
+  if (cs == cudaStreamCaptureStatusInvalidated)
+    return fail(TPO_ERR_CUDA, "the stream's capture has been invalidated");
+  const bool own = cs == cudaStreamCaptureStatusNone;
+  cudaStream_t st = user;  // where the solve's nodes are captured
+  if (own) {
+    if ((rc = capture_streams(nullptr, &st))) return rc;
+    TPO_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  }
+  const double ar = g_alpha_reg[dev];
+  if (std::sqrt(c->f_norm_sq) < 1e-30) {  // reference solver.py:59-63
+    const size_t nn = (size_t)(g->nelx + 1) * (g->nely + 1);
+    if (cudaMemsetAsync(u, 0, 2 * nn * sizeof(double), st) != cudaSuccess)
+      rc = fail(TPO_ERR_CUDA, "memset of u");
+    else
+      k_solve_zero_rhs<<<1, 1, 0, st>>>(out_dev);
+  } else {
+    switch (c->precond) {
+      case TPO_PRECOND_NONE:
+        rc = emit_solve_async<TPO_PRECOND_NONE>(g, c, rho_phys, f, fixed, u, w, out_dev, st, ar);
+        break;
+      case TPO_PRECOND_JACOBI:
+        rc = emit_solve_async<TPO_PRECOND_JACOBI>(g, c, rho_phys, f, fixed, u, w, out_dev, st, ar);
+        break;
+      case TPO_PRECOND_BLOCK_JACOBI:
+        rc = emit_solve_async<TPO_PRECOND_BLOCK_JACOBI>(g, c, rho_phys, f, fixed, u, w, out_dev,
+                                                        st, ar);
+        break;
+      default:
+        rc = emit_solve_async<TPO_PRECOND_NODAL_BLOCK>(g, c, rho_phys, f, fixed, u, w, out_dev, st,
+                                                       ar);
+    }
+  }
+  if (own) {  // not captured by the caller: run the graph once on the stream
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc ? rc : fail(TPO_ERR_CUDA, "capture: %s", cudaGetErrorString(e));
+    }
+    cudaGraphExec_t ex;
+    const cudaError_t ei = cudaGraphInstantiate(&ex, graph, 0);
+    cudaGraphDestroy(graph);
+    TPO_CK(ei);
+    const cudaError_t el = cudaGraphLaunch(ex, user);
+    cudaGraphExecDestroy(ex);  // released by the driver once the launch completes
+    TPO_CK(el);
+  }
+  return rc;
 }
 
 // ------------------------------------------------------------------ sensitivity

@@ -67,6 +67,7 @@ struct TsArgs {
   OuterCtl *octl;
   double *result;         // RAW: optional p.Ap
   int *err;               // TMA timeout flag
+  void *out2;             // RESX: if set, the residual buffer of odd iterations (out: even)
 };
 
 template <typename T, int MODE> struct TsGeom {
@@ -295,7 +296,7 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
         const double rx = f.x - (double)kv.x, ry = f.y - (double)kv.y;
         acc[0] += rx * rx + ry * ry;
         const float2 r32 = make_float2((float)rx, (float)ry);
-        st2<float>(static_cast<float *>(a.out), node, r32);
+        st2<float>(static_cast<float *>((a.out2 && (ctl->it & 1)) ? a.out2 : a.out), node, r32);
         if constexpr (PRE != TPO_PRECOND_BLOCK_JACOBI) {
           // the inner kernels see FP32-stored scales: use the same here
           const double2 z = point_precond<double, PRE>(
@@ -570,6 +571,18 @@ __global__ void __launch_bounds__(UF_THREADS) k_precond_flat(int nx, int ny, int
   precond_flat_run<T, C, PRE>(nx, ny, P, s, mask, r, z, blockIdx.x, gridDim.x);
 }
 
+// the same pass, run only right after an FP64 residual replacement of the
+// mixed form (ctl->since == 0) while the solve goes on: the device-side loop
+// of tpo_pcg_solve_async enqueues it every loop body
+template <typename T, typename C, int PRE>
+__global__ void __launch_bounds__(UF_THREADS) k_precond_gated(const PcgCtl *ctl, int nx, int ny,
+                                                              int P, const T *s,
+                                                              const uint8_t *mask, const T *r,
+                                                              T *z) {
+  if (ctl->status != TPO_SOLVE_RUNNING || ctl->since != 0) return;
+  precond_flat_run<T, C, PRE>(nx, ny, P, s, mask, r, z, blockIdx.x, gridDim.x);
+}
+
 template <typename T, typename C, int PRE, typename X = T>
 __global__ void __launch_bounds__(UF_THREADS) k_update_flat(UpdArgs a) {
   update_flat_run<T, C, PRE, X>(a, blockIdx.x, gridDim.x, gridDim.x, blockIdx.x);
@@ -596,12 +609,14 @@ struct BlkArgs {
   void *z;
   double *part;
   PcgCtl *ctl;
+  int gate;  // INIT: run only right after a residual evaluation (ctl->since == 0)
 };
 
 template <typename T, typename C, bool INIT, int L, typename X = T>
 __global__ void __launch_bounds__(ST_THREADS) k_blockpre(BlkArgs a) {
   PcgCtl *ctl = a.ctl;
   if (ctl->status != TPO_SOLVE_RUNNING) return;
+  if (INIT && a.gate && ctl->since != 0) return;  // no replacement since the last INIT
   const int parity = ctl->it & 1;
   const C alpha = INIT ? C(0) : C(ctl->alpha);
   const T *r_src = static_cast<const T *>(parity ? a.rb : a.ra);

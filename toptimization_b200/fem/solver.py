@@ -3,7 +3,9 @@
 Counterpart of the reference's `src/toptimization/fem/solver.py:27-159`. The
 reference drives CG from a Python loop with two host syncs per iteration; here
 `tpo_pcg_solve` keeps alpha, beta and the stop test on the GPU and the host only
-polls a status word every `poll_every` iterations. The stopping rule, warm
+polls a status word every `poll_every` iterations; `solve_async`
+(`tpo_pcg_solve_async`) runs the whole loop on the device with no host wait,
+so that it can be captured in a CUDA graph. The stopping rule, warm
 start, breakdown test and returned iteration count are the reference's:
 
   * ||f|| < 1e-30             -> u = 0, 0 iterations
@@ -31,6 +33,7 @@ residual is replaced by the FP64 residual f - K u whenever it has dropped by
 
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass
 
 import torch
@@ -86,6 +89,7 @@ class PCGSolver:
             recurrence=RECURRENCE[recurrence])
         lib = _lib.load()
         self._solve = lib.tpo3_pcg_solve if nelz else lib.tpo_pcg_solve
+        self.nelz = nelz
         nbytes = (lib.tpo3_pcg_workspace_bytes(self.grid, self.cfg) if nelz
                   else lib.tpo_pcg_workspace_bytes(self.grid, self.cfg))
         self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
@@ -104,5 +108,40 @@ class PCGSolver:
         _lib.check(self._solve(
             self.grid, self.cfg, _lib.ptr(rho_phys), _lib.ptr(f), _lib.ptr(fixed), _lib.ptr(u),
             _lib.ptr(self.workspace), self.workspace.numel(), res, _lib.stream_handle()))
+        return SolveInfo(_lib.SOLVE_STATUS.get(res.status, str(res.status)), res.iters,
+                         res.outer_iters, res.updates, res.rr)
+
+    RESULT_BYTES = ctypes.sizeof(_lib.TpoSolveResult)
+
+    def result_buffer(self) -> torch.Tensor:
+        """Device memory for one solve result (written by `solve_async`)."""
+        return torch.zeros(self.RESULT_BYTES, dtype=torch.uint8, device=self.device)
+
+    def solve_async(self, rho_phys: torch.Tensor, f: torch.Tensor, fixed: torch.Tensor,
+                    u: torch.Tensor, result: torch.Tensor, warm_start: bool = True) -> None:
+        """`solve`, enqueued on the current stream with no host wait: the PCG
+        loop runs on the device (tpo_pcg_solve_async) and its outcome lands in
+        `result` (a `result_buffer()`; read it with `decode`). Inside a CUDA
+        graph capture the solve becomes part of the graph. 2D grids."""
+        if self.nelz:
+            raise ValueError("3D solves are blocking only (tpo3_pcg_solve)")
+        for t in (rho_phys, f, u):
+            if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
+                raise ValueError("rho_phys, f and u must be contiguous float64 CUDA tensors")
+        if fixed.dtype != torch.uint8:
+            raise ValueError("fixed must be a uint8 per-node mask")
+        if result.numel() * result.element_size() < self.RESULT_BYTES or not result.is_cuda:
+            raise ValueError("result must be a CUDA buffer of at least RESULT_BYTES bytes")
+        self.cfg.warm_start = 1 if warm_start else 0
+        _lib.check(_lib.load().tpo_pcg_solve_async(
+            self.grid, self.cfg, _lib.ptr(rho_phys), _lib.ptr(f), _lib.ptr(fixed), _lib.ptr(u),
+            _lib.ptr(self.workspace), self.workspace.numel(), _lib.ptr(result),
+            _lib.stream_handle()))
+
+    @classmethod
+    def decode(cls, result: torch.Tensor) -> SolveInfo:
+        """The SolveInfo held in a result buffer (copies it to the host)."""
+        raw = bytes(result.reshape(-1)[: cls.RESULT_BYTES].cpu().numpy().tobytes())
+        res = _lib.TpoSolveResult.from_buffer_copy(raw)
         return SolveInfo(_lib.SOLVE_STATUS.get(res.status, str(res.status)), res.iters,
                          res.outer_iters, res.updates, res.rr)

@@ -155,6 +155,61 @@ class SimpDesign:
         return self.rho.cpu().numpy()
 
 
+class CapturedDesign(SimpDesign):
+    """A SimpDesign whose OC iteration is one CUDA graph: the filters, the
+    asynchronous PCG solve (its loop a device-side while node,
+    `PCGSolver.solve_async`), the sensitivity and the OC update are captured
+    once and replayed every iteration; the host reads the five scalars and the
+    solve result after each replay. The same kernels in the same order as
+    `SimpDesign.step`, so the same results, for every 2D form (FP64 and mixed,
+    every preconditioner, both filter types). The first OC iteration (the cold
+    start) runs uncaptured; it also sets up the launch plans."""
+
+    def __init__(self, problem, device=None, precision: str | None = None,
+                 preconditioner: str | None = None):
+        if problem.dim != 2:
+            raise ValueError("engine='graph' runs 2D designs")
+        super().__init__(problem, device=device, precision=precision,
+                         preconditioner=preconditioner)
+        self.result = self.solver.result_buffer()
+        self.graph = None
+
+    def _enqueue(self, warm: bool) -> None:
+        pr = self.problem
+        if pr.filter_type == "density":
+            filt.density_filter(self.grid, pr.rmin, self.rho, self.rho_phys)
+            self.solver.solve_async(self.rho_phys, self.f, self.fixed, self.u, self.result, warm)
+            K.sensitivity(self.grid, self.rho_phys, self.u, self.dc, self.scalars[0:1],
+                          self.sens_ws)
+            filt.density_filter(self.grid, pr.rmin, self.dc, self.dc_filt)
+        else:
+            self.solver.solve_async(self.rho, self.f, self.fixed, self.u, self.result, warm)
+            K.sensitivity(self.grid, self.rho, self.u, self.dc, self.scalars[0:1], self.sens_ws)
+            filt.sensitivity_filter(self.grid, pr.rmin, self.rho, self.dc, self.dc_filt)
+        oc_mod.oc_update(self.grid, pr.volfrac, pr.move_limit, self.rho, self.dc_filt,
+                         self.rho, self.scalars[1:5], self.oc_ws)
+
+    def step(self) -> IterationRecord:
+        t0 = time.perf_counter()
+        self.it += 1
+        with torch.cuda.device(self.device):
+            if self.it == 1:
+                self._enqueue(False)
+            else:
+                if self.graph is None:
+                    side = torch.cuda.Stream(self.device)
+                    side.wait_stream(torch.cuda.current_stream(self.device))
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=side, capture_error_mode="thread_local"):
+                        self._enqueue(True)
+                    self.graph = g
+                self.graph.replay()
+            c, change, vol, _lam, _steps = self.scalars.cpu().tolist()
+            info = PCGSolver.decode(self.result)
+        return IterationRecord(self.it, c, vol, change, info.iters, info,
+                               time.perf_counter() - t0)
+
+
 class GraphDesign:
     """One design run through the batched engine (`toptimization_b200.batch`)
     as a batch of one: each OC iteration is a single CUDA graph launch in which
@@ -215,16 +270,23 @@ def run(problem, backend: str = "auto", live_viz: bool = True,
     (simp.py:213-214). `live_viz` is accepted for compatibility; there is no
     window (headless). `precision` overrides `problem.precision`
     ("fp64" | "mixed"); `history` (optional) receives every per-iteration record.
-    `engine="graph"` runs each OC iteration as one CUDA graph (mixed precision,
-    density filter, point preconditioner; see `GraphDesign`).
+    `engine="graph"` runs each OC iteration as one CUDA graph with the PCG
+    loop on the device, any 2D form (`CapturedDesign`); `engine="batch"` runs
+    the design through the batched engine as a batch of one (mixed precision,
+    density filter, point preconditioner; `GraphDesign`).
     """
     _check_backend(backend)
     pr = problem
     if engine == "graph":
         if pr.dim != 2:
             raise ValueError("engine='graph' runs 2D designs")
+        design = CapturedDesign(pr, device=device, precision=precision,
+                                preconditioner=preconditioner)
+    elif engine == "batch":
+        if pr.dim != 2:
+            raise ValueError("engine='batch' runs 2D designs")
         if (precision or pr.precision) != "mixed":
-            raise ValueError("engine='graph' runs the mixed-precision form")
+            raise ValueError("engine='batch' runs the mixed-precision form")
         design = GraphDesign(pr, device=device, preconditioner=preconditioner)
     elif engine == "direct":
         design = SimpDesign(pr, device=device, precision=precision,
