@@ -11,9 +11,14 @@ PCG solve, sensitivity, dc filter, OC bisection). W untimed steps on one
 design, then K timed steps -- OC iterations 1..K -- of a fresh design from the
 initial density, each bracketed by CUDA events on the launching stream, with a
 256 MiB write between steps to flush L2. The headline `value` is the mixed
-form (FP32-stored inner PCG inside FP64 refinement); the plain FP64 form is
-timed on the same OC iterations beside it, and `e2e` runs the same OC
-iterations through simp.run() with host buffers. The line also carries a
+form (FP32-stored inner PCG inside FP64 refinement) through the CUDA-graph
+engine (simp.run(engine="graph"): each OC iteration one graph, the PCG loop
+a device-side while node); the plain FP64 form is timed on the same OC
+iterations and engine beside it, the host-polled engine ("direct") on the
+same iterations too, and `e2e` runs the same OC iterations through
+simp.run(engine="graph") with host buffers. Per-kernel device times come
+from the host-polled path (the library brackets every PCG launch with
+events), one OC iteration per form. The line also carries a
 whole, measured (not extrapolated) comparison on the 400x200 cantilever:
 GPU forms against the CPU port on the host cores.
 
@@ -64,6 +69,7 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-direct", action="store_true")
     ap.add_argument("--case", choices=["pcg", "matvec"], default=None,
                     help="profiling case: one PCG solve on the bridge capped at --cg-iters, "
                          "or 5 stiffness applications (FP64) on the bridge")
@@ -374,7 +380,7 @@ def run_ours(args):
 
     from toptimization_b200 import _lib
     from toptimization_b200.csrc import build as csrc_build
-    from toptimization_b200.optimizer.simp import SimpDesign, run
+    from toptimization_b200.optimizer.simp import CapturedDesign, SimpDesign, run
     if rank == 0:
         csrc_build.build()
     replicas.barrier(rk)  # the library is built once, by rank 0
@@ -389,44 +395,66 @@ def run_ours(args):
     def max_over_ranks(x: float) -> float:
         return replicas.max_over_ranks(x, rk, dev)
 
-    def warm_then_fresh(precision):
+    def warm_then_fresh(precision, cls=SimpDesign):
         """W untimed OC iterations on a throwaway design (kernel load, launch
         plans, allocator), then a fresh design from the initial density: the
         timed steps are OC iterations 1..K, the window the e2e run covers."""
         if args.warmup:
-            w = SimpDesign(pr, device=dev, precision=precision, preconditioner=PRECONDITIONER)
+            w = cls(pr, device=dev, precision=precision, preconditioner=PRECONDITIONER)
             for _ in range(args.warmup):
                 w.step()
             torch.cuda.synchronize()
             del w
-        return SimpDesign(pr, device=dev, precision=precision, preconditioner=PRECONDITIONER)
+        return cls(pr, device=dev, precision=precision, preconditioner=PRECONDITIONER)
 
-    # ---- mixed (headline), timed
-    mixed = warm_then_fresh("mixed")
+    # ---- mixed (headline), timed, through the CUDA-graph engine (each OC
+    # iteration one graph, the PCG loop on the device: simp.run(engine="graph"))
+    mixed = warm_then_fresh("mixed", CapturedDesign)
     barrier()
-    lib.tpo_profile_reset()
     with ClockSampler(local) as clocks:
         times_m, recs_m = time_steps(mixed, args.steps, 0, flush, torch)
     barrier()
-    launches = _lib.profile_read()["launches"]
+    launches = sum(r.launches for r in recs_m)
     t_mixed = max_over_ranks(sum(times_m))
     clock_info = clocks.summary()
     rho_mixed = mixed.density()
-
-    # ---- per-kernel timing pass (events around every PCG launch), same design
-    kern_mixed = profile_pass(mixed, lib, _lib, torch)
     del mixed
 
-    # ---- plain FP64, same steps
+    # ---- per-kernel device times (events around every PCG launch, recorded by
+    # the library) on the host-polled path, same kernels: one OC iteration
+    def kernel_pass(precision):
+        d = SimpDesign(pr, device=dev, precision=precision, preconditioner=PRECONDITIONER)
+        out = profile_pass(d, lib, _lib, torch)
+        del d
+        return out
+    kern_mixed = kernel_pass("mixed")
+
+    # ---- the host-polled path (simp.run(engine="direct")), same OC iterations
+    direct = None
+    if not args.no_direct:
+        dd = warm_then_fresh("mixed")
+        barrier()
+        times_x, recs_x = time_steps(dd, args.steps, 0, flush, torch)
+        barrier()
+        t_x = max_over_ranks(sum(times_x))
+        direct = {"value": round(world * args.steps / (t_x / 1e3), 4),
+                  "ms_per_step": round(t_x / args.steps, 3),
+                  "engine": "simp.run(engine='direct'): host polls the PCG status",
+                  "same_results_as_graph": [r.compliance for r in recs_x] ==
+                                           [r.compliance for r in recs_m]}
+        del dd
+
+    # ---- plain FP64, same OC iterations, same engine
     fp64 = None
     if not args.no_fp64:
-        d64 = warm_then_fresh("fp64")
+        d64 = warm_then_fresh("fp64", CapturedDesign)
         barrier()
         times_d, recs_d = time_steps(d64, args.steps, 0, flush, torch)
         barrier()
         t_d = max_over_ranks(sum(times_d))
         rho_fp64 = d64.density()
-        kern_fp64 = profile_pass(d64, lib, _lib, torch)
+        del d64
+        kern_fp64 = kernel_pass("fp64")
         cd = np.array([r.compliance for r in recs_d])
         fp64 = {"value": round(world * args.steps / (t_d / 1e3), 4),
                 "ms_per_step": round(t_d / args.steps, 3),
@@ -434,7 +462,6 @@ def run_ours(args):
                 "cg_iters": [r.cg_iters for r in recs_d],
                 "compliance": [float(x) for x in cd], "kernels": kern_fp64,
                 "density_max_abs_mixed_vs_fp64": float(np.abs(rho_mixed - rho_fp64).max())}
-        del d64
 
     # ---- matvec roofline (FP64 and FP32 operator alone)
     mv64 = time_matvec(pr, torch.float64, torch)
@@ -450,7 +477,7 @@ def run_ours(args):
         barrier()
         t0 = time.perf_counter()
         run(pr_e, backend="cuda", live_viz=False, precision="mixed", verbose=False, save=False,
-            viz_callback=lambda rho, it, c, v: got.append(rho.nbytes))
+            viz_callback=lambda rho, it, c, v: got.append(rho.nbytes), engine="graph")
         torch.cuda.synchronize()
         t_e = max_over_ranks(time.perf_counter() - t0)
         n_it = pr_e.max_iter
@@ -458,7 +485,7 @@ def run_ours(args):
         e2e = {"value": round(world * n_it / t_e, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d / n_it),
                "d2h_bytes_per_step": int(np.mean(got)) + 5 * 8,
-               "note": (f"simp.run() from a host Problem to the host density: OC iterations "
+               "note": (f"simp.run(engine='graph') from a host Problem to the host density: OC iterations "
                         f"1..{n_it} from the initial design, the same iterations as `value`, "
                         "plus setup, H2D of loads and BCs, per-iteration D2H of the density "
                         "to a viz_callback and of 5 scalars")}
@@ -507,6 +534,8 @@ def run_ours(args):
         rel = [abs(a - b) / abs(b) for a, b in zip(line["mixed"]["compliance"], fp64["compliance"])]
         line["compliance_rel_err_mixed_vs_fp64"] = max(rel)
         line["density_max_abs_mixed_vs_fp64"] = fp64["density_max_abs_mixed_vs_fp64"]
+    if direct is not None:
+        line["mixed_direct_engine"] = direct
     if e2e is not None:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu:

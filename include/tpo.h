@@ -114,6 +114,9 @@ typedef struct tpo_solve_result {
   int32_t outer_iters;  /* mixed: refinement steps taken (FP64: 1) */
   int32_t updates;      /* PCG updates actually performed */
   double rr;            /* last ||r||^2 seen (mixed: true FP64 residual) */
+  int32_t launches;     /* kernels the solve ran (tpo_pcg_solve_async: each loop
+                           body's kernels counted every time the body ran) */
+  int32_t bodies;       /* tpo_pcg_solve_async: device loop bodies run (else 0) */
 } tpo_solve_result;
 
 int tpo_version(void);

@@ -2,7 +2,9 @@
 
 Run in a container that has the reference checkout (not on the GPU machines):
 
-    python tests/golden/make_golden.py --reference /root/reference/src
+    python tests/golden/make_golden.py --reference <reference checkout>/src
+
+(or set TPO_REFERENCE_SRC to that directory)
 
 What is recorded, all from the reference's own code:
   boundary.npz        Ke (Q4, H8), Ke_inv/alpha, edof (4x3), the fixed-DOF and
@@ -30,6 +32,7 @@ import argparse
 import contextlib
 import io
 import multiprocessing as mp
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -316,9 +319,12 @@ def _run(args) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference/src")
+    ap.add_argument("--reference", default=os.environ.get("TPO_REFERENCE_SRC"),
+                    help="the src/ directory of a reference checkout")
     ap.add_argument("--only", default="")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("give --reference or set TPO_REFERENCE_SRC")
     ref_src = a.reference
     ref_examples = Path(ref_src).parent / "examples"
     ctx = mp.get_context("spawn")

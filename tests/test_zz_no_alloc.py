@@ -54,6 +54,34 @@ def test_noalloc_matches_workspace_entry_point(tpo_built, nx, ny):
         assert c_b.item() == pytest.approx(c_a.item(), rel=1e-13), f"call {call}"
 
 
+def test_noalloc_second_call_on_another_stream(tpo_built):
+    """A call on a new stream, after the first call (on the default stream)
+    has finished: the scratch's ticket starts at zero again, so the result
+    still equals the workspace entry point's."""
+    Ke = compute_Ke_2d(1.0, 0.3)
+    inv, alpha = regularized_inverse(Ke)
+    _lib.ensure_stiffness(Ke, inv, alpha)
+    nx, ny = 256, 96
+    g = _lib.grid(nx, ny, 1e-9, 3.0)
+    rng = np.random.default_rng(5)
+    rho = torch.from_numpy(rng.uniform(0.001, 1.0, nx * ny)).cuda()
+    u = torch.from_numpy(rng.standard_normal(2 * (nx + 1) * (ny + 1))).cuda()
+    dc_a, dc_b = torch.empty_like(rho), torch.empty_like(rho)
+    c_a = torch.empty(1, dtype=torch.float64, device="cuda")
+    c_b = torch.empty(1, dtype=torch.float64, device="cuda")
+    _lib.check(_call_workspace(g, rho, u, dc_a, c_a))
+    _lib.check(_call_noalloc(g, rho, u, dc_b, c_b))
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        dc_b.zero_()
+        _lib.check(_call_noalloc(g, rho, u, dc_b, c_b))
+    s.synchronize()
+    a, b = dc_a.cpu().numpy(), dc_b.cpu().numpy()
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max()
+    assert c_b.item() == pytest.approx(c_a.item(), rel=1e-13)
+
+
 def test_noalloc_rejects_grids_beyond_the_scratch(tpo_built):
     Ke = compute_Ke_2d(1.0, 0.3)
     inv, alpha = regularized_inverse(Ke)

@@ -48,7 +48,8 @@ class TpoSolveCfg(ctypes.Structure):
 
 class TpoSolveResult(ctypes.Structure):
     _fields_ = [("status", c_int32), ("iters", c_int32), ("outer_iters", c_int32),
-                ("updates", c_int32), ("rr", c_double)]
+                ("updates", c_int32), ("rr", c_double), ("launches", c_int32),
+                ("bodies", c_int32)]
 
 
 class TpoProfile(ctypes.Structure):
@@ -192,6 +193,14 @@ def grid3(nelx: int, nely: int, nelz: int, e_min: float, penalty: float) -> TpoG
 
 def is3d(g) -> bool:
     return isinstance(g, TpoGrid3)
+
+
+def launch_count() -> int:
+    """Kernel launches this library has enqueued since the last
+    tpo_profile_reset (a counter on the host; graph replays do not add)."""
+    out = TpoProfile()
+    check(load().tpo_profile_read(ctypes.byref(out)))
+    return int(out.launches)
 
 
 def ptr(t) -> int:

@@ -941,7 +941,8 @@ __global__ void k_solve_cond(const PcgCtl *ctl, const OuterCtl *octl, uint32_t *
 
 // The host epilogues of pcg_fp64 / pcg_single / pcg_mixed, on the device.
 __global__ void k_solve_result(const PcgCtl *ctl, const OuterCtl *octl, const uint32_t *bodies,
-                               uint32_t max_bodies, int max_iter, tpo_solve_result *out) {
+                               uint32_t max_bodies, int max_iter, int n_fixed, int n_body,
+                               tpo_solve_result *out) {
   int status;
   tpo_solve_result r{};
   if (octl) {
@@ -967,6 +968,8 @@ __global__ void k_solve_result(const PcgCtl *ctl, const OuterCtl *octl, const ui
            (octl ? octl->status == TPO_SOLVE_RUNNING : ctl->status == TPO_SOLVE_RUNNING))
     status = TPO_SOLVE_LOOP_LIMIT;
   r.status = status;
+  r.bodies = (int32_t)*bodies;
+  r.launches = n_fixed + (int32_t)*bodies * n_body;
   *out = r;
 }
 
@@ -974,6 +977,7 @@ __global__ void k_solve_zero_rhs(tpo_solve_result *out) {
   tpo_solve_result r{};
   r.status = TPO_SOLVE_ZERO_RHS;
   r.outer_iters = 1;
+  r.launches = 1;
   *out = r;
 }
 
@@ -1002,7 +1006,7 @@ int capture_streams(cudaStream_t *body, cudaStream_t *cap) {
 // the stream's later work ordered after the node.
 template <typename BodyFn>
 int add_while_loop(cudaStream_t st, BodyFn emit, const PcgCtl *ctl, const OuterCtl *octl,
-                   uint32_t *bodies, uint32_t max_bodies) {
+                   uint32_t *bodies, uint32_t max_bodies, int *n_body) {
   cudaStreamCaptureStatus cst;
   cudaGraph_t g = nullptr;
   const cudaGraphNode_t *deps = nullptr;
@@ -1026,7 +1030,9 @@ int add_while_loop(cudaStream_t st, BodyFn emit, const PcgCtl *ctl, const OuterC
   if (rc) return rc;
   TPO_CK(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
                                        cudaStreamCaptureModeRelaxed));
+  const int64_t l0 = g_launches.load();
   rc = emit(bs);
+  *n_body = (int)(g_launches.load() - l0) + 1;  // + the condition kernel
   if (!rc) {
     k_solve_cond<<<1, 1, 0, bs>>>(ctl, octl, bodies, max_bodies, h);
     if (cudaPeekAtLastError() != cudaSuccess) rc = fail(TPO_ERR_CUDA, "loop condition launch");
@@ -1053,6 +1059,8 @@ int emit_solve_async(const tpo_grid *g, const tpo_solve_cfg *c, const double *rh
   const double fn = std::sqrt(c->f_norm_sq);
   const double tol_sq = (c->tol * fn) * (c->tol * fn);
   const dim3 sg = flat_grid((size_t)nx * P, 256, sm_count() * 16);
+  const int64_t l0 = g_launches.load();
+  int n_body = 0;
   int rc = pack_inputs(g, w, f, fixed, u, c->warm_start != 0, st);
   if (rc) return rc;
   if ((rc = zero_vectors(w, NN, st))) return rc;
@@ -1112,7 +1120,7 @@ int emit_solve_async(const tpo_grid *g, const tpo_solve_cfg *c, const double *rh
       }
       return TPO_OK;
     };
-    rc = add_while_loop(st, body, w.ctl, w.octl, w.bodies, max_bodies);
+    rc = add_while_loop(st, body, w.ctl, w.octl, w.bodies, max_bodies, &n_body);
   } else {
     k_scales<<<sg, 256, 0, st>>>(nx, ny, P, rho, g->e_min, g->penalty, alpha_reg, w.s64, nullptr,
                                  block ? w.w64 : nullptr, nullptr);
@@ -1136,7 +1144,7 @@ int emit_solve_async(const tpo_grid *g, const tpo_solve_cfg *c, const double *rh
         }
         return TPO_OK;
       };
-      rc = add_while_loop(st, body, w.ctl, nullptr, w.bodies, max_bodies);
+      rc = add_while_loop(st, body, w.ctl, nullptr, w.bodies, max_bodies, &n_body);
     } else {
       BlkArgs b{};
       b.nx = nx; b.ny = ny; b.P = P;
@@ -1172,13 +1180,15 @@ int emit_solve_async(const tpo_grid *g, const tpo_solve_cfg *c, const double *rh
         }
         return TPO_OK;
       };
-      rc = add_while_loop(st, body, w.ctl, nullptr, w.bodies, max_bodies);
+      rc = add_while_loop(st, body, w.ctl, nullptr, w.bodies, max_bodies, &n_body);
     }
   }
   if (rc) return rc;
   if ((rc = unpack_solution(g, w, u, st))) return rc;
+  // kernels outside the loop: those enqueued so far less one body's, plus this one
+  const int n_fixed = (int)(g_launches.load() - l0) - (n_body - 1) + 1;
   k_solve_result<<<1, 1, 0, st>>>(w.ctl, mixed ? w.octl : nullptr, w.bodies, max_bodies,
-                                  c->max_iter, out);
+                                  c->max_iter, n_fixed, n_body, out);
   TPO_CK_LAUNCH();
   return TPO_OK;
 }
@@ -1406,6 +1416,8 @@ int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_p
   }
   const double ar = g_alpha_reg[dev];
   const bool mixed = c->precision == TPO_PRECISION_MIXED;
+  const int64_t l0 = g_launches.load();
+  auto dispatch = [&]() -> int {
   if (w.single) {
     switch (c->precond) {
       case TPO_PRECOND_NONE:
@@ -1432,6 +1444,10 @@ int tpo_pcg_solve(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_p
                  ? pcg_mixed<TPO_PRECOND_NODAL_BLOCK>(g, c, rho_phys, f, fixed, u, w, out, st, ar)
                  : pcg_fp64<TPO_PRECOND_NODAL_BLOCK>(g, c, rho_phys, f, fixed, u, w, out, st, ar);
   }
+  };
+  rc = dispatch();
+  out->launches = (int32_t)(g_launches.load() - l0);
+  return rc;
 }
 
 int tpo_pcg_solve_async(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho_phys,
@@ -1513,7 +1529,9 @@ int tpo_sensitivity(const tpo_grid *g, const double *rho_phys, const double *u, 
   if ((rc = need_stiffness(&dev))) return rc;
   if (!rho_phys || !u || !dc || !compliance_out || !ws)
     return fail(TPO_ERR_ARGS, "NULL pointer argument");
-  if (!aligned(u, 16) || !aligned(ws, kAlign)) return fail(TPO_ERR_ARGS, "misaligned pointer");
+  if (!aligned(u, 16) || !aligned(ws, kAlign) || !aligned(rho_phys, 8) || !aligned(dc, 8) ||
+      !aligned(compliance_out, 8))
+    return fail(TPO_ERR_ARGS, "misaligned pointer (u 16 B, doubles 8 B, workspace 256 B)");
   if (ws_bytes < tpo_sensitivity_workspace_bytes(g))
     return fail(TPO_ERR_WORKSPACE, "workspace too small");
   cudaStream_t st = static_cast<cudaStream_t>(s);
@@ -1546,7 +1564,8 @@ int tpo_sensitivity_noalloc(const tpo_grid *g, const double *rho_phys, const dou
   int dev;
   if ((rc = need_stiffness(&dev))) return rc;
   if (!rho_phys || !u || !dc || !compliance_out) return fail(TPO_ERR_ARGS, "NULL pointer argument");
-  if (!aligned(u, 16)) return fail(TPO_ERR_ARGS, "misaligned pointer");
+  if (!aligned(u, 16) || !aligned(rho_phys, 8) || !aligned(dc, 8) || !aligned(compliance_out, 8))
+    return fail(TPO_ERR_ARGS, "misaligned pointer (u 16 B, doubles 8 B)");
   const dim3 gr((g->nely + S_THREADS - 1) / S_THREADS, (g->nelx + SL - 1) / SL, 1);
   const size_t nb = (size_t)gr.x * gr.y;
   if (nb > kSensMaxPartials)

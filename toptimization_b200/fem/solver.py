@@ -51,6 +51,8 @@ class SolveInfo:
     outer_iters: int
     updates: int
     rr: float
+    launches: int = 0  # kernels the solve ran
+    bodies: int = 0    # device loop bodies (asynchronous solve)
 
     @property
     def converged(self) -> bool:
@@ -109,7 +111,7 @@ class PCGSolver:
             self.grid, self.cfg, _lib.ptr(rho_phys), _lib.ptr(f), _lib.ptr(fixed), _lib.ptr(u),
             _lib.ptr(self.workspace), self.workspace.numel(), res, _lib.stream_handle()))
         return SolveInfo(_lib.SOLVE_STATUS.get(res.status, str(res.status)), res.iters,
-                         res.outer_iters, res.updates, res.rr)
+                         res.outer_iters, res.updates, res.rr, res.launches, res.bodies)
 
     RESULT_BYTES = ctypes.sizeof(_lib.TpoSolveResult)
 
@@ -144,4 +146,4 @@ class PCGSolver:
         raw = bytes(result.reshape(-1)[: cls.RESULT_BYTES].cpu().numpy().tobytes())
         res = _lib.TpoSolveResult.from_buffer_copy(raw)
         return SolveInfo(_lib.SOLVE_STATUS.get(res.status, str(res.status)), res.iters,
-                         res.outer_iters, res.updates, res.rr)
+                         res.outer_iters, res.updates, res.rr, res.launches, res.bodies)
