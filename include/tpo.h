@@ -122,6 +122,14 @@ typedef struct tpo_solve_result {
 int tpo_version(void);
 const char *tpo_last_error_string(void);
 
+/* Failure tests only; no counterpart in the reference. The next stencil
+ * launch of this process withholds the bulk copies of its column group
+ * `group` (in every CTA), so that the bounded waits for it run out (about
+ * 1.3 s each): the kernel sets its error flag, lets its other copies land
+ * and returns, and the solve reports TPO_ERR_TIMEOUT (tpo_pcg_solve) or
+ * TPO_SOLVE_TIMEOUT (tpo_pcg_solve_async). The device stays usable. */
+int tpo_test_withhold_stage(int32_t group);
+
 /* Element stiffness (8x8 Q4, row-major), its regularised inverse and the
  * regulariser (reference fem/fields.py:133-143), copied to constant memory of
  * the CURRENT device. Must be called once per device before any kernel. */

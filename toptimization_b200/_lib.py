@@ -99,6 +99,7 @@ _SIGS = {
     "tpo_pcg_solve": (c_int, [POINTER(TpoGrid), POINTER(TpoSolveCfg), c_void_p, c_void_p,
                               c_void_p, c_void_p, c_void_p, c_size_t, POINTER(TpoSolveResult),
                               c_void_p]),
+    "tpo_test_withhold_stage": (c_int, [c_int32]),
     "tpo_pcg_solve_async": (c_int, [POINTER(TpoGrid), POINTER(TpoSolveCfg), c_void_p,
                                     c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p,
                                     c_void_p]),

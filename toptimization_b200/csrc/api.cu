@@ -169,6 +169,9 @@ int sm_count() {
 // Stencil launch configuration per kernel instantiation: dynamic shared
 // memory (set once), resident CTAs per SM, and the strip length that makes
 // the grid close to one full wave.
+// failure tests (tpo_test_withhold_stage): group + 1 for the next stencil launch
+std::atomic<int> g_withhold1{0};
+
 #ifndef TPO_MIN_STRIP
 #define TPO_MIN_STRIP 8
 #endif
@@ -210,7 +213,9 @@ template <typename T, typename C, int MODE, int PRE> struct StencilCfg {
   }
   static int launch(cudaStream_t st, const TsArgs &a, int nx, int ny) {
     const Plan pl = plan(nx, ny);
-    k_tstencil<T, C, MODE, PRE, G, NG><<<pl.grid, TS_THREADS, SMEM, st>>>(a, pl.L);
+    TsArgs b = a;
+    b.withhold1 = g_withhold1.exchange(0);  // 0 unless a failure test armed it
+    k_tstencil<T, C, MODE, PRE, G, NG><<<pl.grid, TS_THREADS, SMEM, st>>>(b, pl.L);
     return TPO_OK;
   }
   static int max_ctas(int nx, int ny) {
@@ -801,8 +806,11 @@ int pcg_mixed(const tpo_grid *g, const tpo_solve_cfg *c, const double *rho, cons
           nx, ny, P, w.s32, w.mask, w.fra, w.fz);
       TPO_CK_LAUNCH();
     }
+    int err = 0;  // a pipeline wait of the residual kernels ran out
     TPO_CK(cudaMemcpyAsync(&oh, w.octl, sizeof(OuterCtl), cudaMemcpyDeviceToHost, st));
+    TPO_CK(cudaMemcpyAsync(&err, &w.ctl->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     TPO_CK(cudaStreamSynchronize(st));
+    if (err) return fail(TPO_ERR_TIMEOUT, "a TMA pipeline wait ran out of time");
     if (oh.status != TPO_SOLVE_RUNNING) {
       status = oh.status;
       break;
@@ -1268,6 +1276,12 @@ static int apply_impl(const tpo_grid *g, const T *elem, bool from_density, const
 extern "C" {
 
 int tpo_version(void) { return 1; }
+
+int tpo_test_withhold_stage(int32_t group) {
+  if (group < 0) return fail(TPO_ERR_ARGS, "group must be >= 0");
+  g_withhold1.store(group + 1);
+  return TPO_OK;
+}
 
 const char *tpo_last_error_string(void) { return g_err.c_str(); }
 

@@ -149,11 +149,10 @@ __global__ void __launch_bounds__(CG_THREADS) k_cgstep(CgArgs A, int L) {
         issue(k);
         issued = k + 1;
       }
-      if (!ok) {
-        // let the copies this CTA started land before it exits
-        for (int k = (issued > NG ? issued - NG : 0); k < issued; ++k)
-          mbar_wait_bounded(&full[k % NG], (k / NG) & 1, nullptr, 0);
-      }
+      // let the copies this CTA started land before it exits (the consumers
+      // wait for every column too, but one whose wait ran out stops waiting)
+      for (int k = (issued > NG ? issued - NG : 0); k < issued; ++k)
+        mbar_wait_bounded(&full[k % NG], (k / NG) & 1, nullptr, 0);
     }
   } else {
 

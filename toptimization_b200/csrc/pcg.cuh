@@ -68,6 +68,7 @@ struct TsArgs {
   double *result;         // RAW: optional p.Ap
   int *err;               // TMA timeout flag
   void *out2;             // RESX: if set, the residual buffer of odd iterations (out: even)
+  int withhold1;          // failure tests only: g + 1 withholds the copies of column group g
 };
 
 template <typename T, int MODE> struct TsGeom {
@@ -136,6 +137,7 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
   // and the producer refills with a lag of one group, so warps may drift
   // apart by a group without waiting for each other.
   auto issue = [&](int g) {
+    if (g + 1 == a.withhold1) return;  // failure tests: the group's wait must run out
     unsigned char *sb = smem + (g % NG) * SLOT;
     unsigned bytes = 0;
     for (int k = 0; k < G; ++k) {
@@ -188,9 +190,12 @@ __device__ __forceinline__ void tstencil_run(const TsArgs &a, int L, int bx, int
         issue(g);
         issued = g + 1;
       }
-      if (!ok)  // let the copies this CTA started land before it exits
-        for (int g = (issued > NG ? issued - NG : 0); g < issued; ++g)
-          mbar_wait_bounded(&full[g % NG], (g / NG) & 1, nullptr, 0);
+      // Let the copies this CTA started land before it exits: the consumer
+      // warps wait for every group too, but one whose wait ran out stops
+      // waiting, so the producer confirms the last group of each slot itself
+      // (bounded; at once in a normal run).
+      for (int g = (issued > NG ? issued - NG : 0); g < issued; ++g)
+        mbar_wait_bounded(&full[g % NG], (g / NG) & 1, nullptr, 0);
     }
   } else {
 
