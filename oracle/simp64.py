@@ -196,14 +196,19 @@ class SolveResult:
     rr: float
 
 
+def _dot(a, b):
+    return float(a @ b)
+
+
 def pcg(mesh, scale, f, u0, tol, max_iter, precond="jacobi",
-        assemble: bool = True) -> SolveResult:
+        assemble: bool = True, dot=_dot) -> SolveResult:
     """PCG exactly as the reference drives it (`fem/solver.py:27-159`):
     warm start with fixed DOFs zeroed, true initial residual, breakdown when
     |p.Ap| < 1e-30, recursive-residual stop ||r||^2 < (tol ||f||)^2 tested
     before the direction update, beta = rz_new/(rz_old + 1e-60). Returns the
     reference's count (it+1 on convergence, max_iter otherwise -- also after a
-    breakdown)."""
+    breakdown). `dot` computes the iteration's dot products (a test swaps in
+    other roundings of the same sums)."""
     f_norm = math.sqrt(float(f @ f))
     if f_norm < 1e-30:
         return SolveResult(np.zeros_like(f), 0, "zero_rhs", 0.0)
@@ -215,19 +220,19 @@ def pcg(mesh, scale, f, u0, tol, max_iter, precond="jacobi",
     r = f - K @ u
     z = M(r)
     p = z.copy()
-    rz_old = float(r @ z)
-    rr = float(r @ r)
+    rz_old = dot(r, z)
+    rr = dot(r, r)
     for it in range(max_iter):
         Ap = K @ p
-        pAp = float(p @ Ap)
+        pAp = dot(p, Ap)
         if abs(pAp) < 1e-30:
             return SolveResult(u, max_iter, "breakdown", rr)
         alpha = rz_old / pAp
         u += alpha * p
         r -= alpha * Ap
         z = M(r)
-        rz_new = float(r @ z)
-        rr = float(r @ r)
+        rz_new = dot(r, z)
+        rr = dot(r, r)
         if rr < tol_sq:
             return SolveResult(u, it + 1, "converged", rr)
         beta = rz_new / (rz_old + 1e-60)
@@ -340,11 +345,12 @@ class RunResult:
     status: list
 
 
-def run(problem, max_iter=None, callback=None) -> RunResult:
+def run(problem, max_iter=None, callback=None, dot=_dot) -> RunResult:
     """The SIMP loop of `optimizer/simp.py:108-109,141-219` (2D or 3D): density filter ->
     PCG on the physical density (warm start from it > 1) -> sensitivity ->
     dc projection -> OC on the design density -> volume; early stop when
-    it > 5 and change < tol. The sensitivity-filter branch (:174-189) too."""
+    it > 5 and change < tol. The sensitivity-filter branch (:174-189) too.
+    `dot` is passed to the PCG."""
     pr = problem
     Ke = compute_Ke(pr.E, pr.nu, pr.dim)
     nelz = pr.nelz if pr.dim == 3 else 0
@@ -361,7 +367,7 @@ def run(problem, max_iter=None, callback=None) -> RunResult:
         phys = density_filter(H, Hs, rho) if pr.filter_type == "density" else rho
         scale = simp_scale(phys, pr.E_min, pr.penalty)
         res = pcg(mesh, scale, f, u_prev if it > 1 else np.zeros(mesh.n_dofs),
-                  pr.cg_tol, pr.max_cg_iter, pr.preconditioner)
+                  pr.cg_tol, pr.max_cg_iter, pr.preconditioner, dot=dot)
         if res.status != "zero_rhs":
             u_prev = res.u
         dc, c = sensitivity(mesh, res.u, phys, pr.E_min, pr.penalty)
