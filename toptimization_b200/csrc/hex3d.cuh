@@ -10,9 +10,13 @@
 //   element (ex, ey, ez) -> (ex*nely + ey)*nelz + ez
 //   fixed mask           -> uint8 per node, bit0/1/2 = x/y/z fixed
 //
-// Every nodal operator is a gather: one thread per node sums the rows of its
-// (up to) eight elements. Thread n reads the 27-node neighbourhood once (3
-// values each) and keeps one partial 3-vector per incident element,
+// The stiffness applications (matvec, PCG direction, first residual) run
+// element-centric with a structured H8 operator (k_hex_elem, below) when the
+// stiffness has the isotropic unit-cube form, which tpo_set_stiffness3
+// checks. The element-block preconditioner, and any other stiffness, use a
+// gather: one thread per node sums the rows of its (up to) eight elements.
+// Thread n reads the 27-node neighbourhood once (3 values each) and keeps one
+// partial 3-vector per incident element,
 //   y_k += Ke[3a+c][3b+j] v_m[j]      (a: the node's corner in element k,
 //                                       b: neighbour m's corner),
 // then scales each by its element weight: 64 node pairs x 9 multiply-adds +
@@ -543,6 +547,375 @@ __global__ void __launch_bounds__(HT_THREADS, 3) k_hex_tile(Hex3Args a, int xc) 
     if (!finite(acc[0]) || !finite(acc[1])) ctl->status = TPO_SOLVE_NONFINITE;
   } else {
     finish_update(ctl, acc[0], acc[1]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Structured H8 operator. For the unit-cube trilinear element of an isotropic
+// material with exact (2x2x2 Gauss) integration, f = w Ke u follows from the
+// element's trilinear modal coefficients:
+// * an 8-point Walsh-Hadamard transform maps each displacement component's
+//   corner values onto the monomials 1, xi, eta, zeta, xi eta, eta zeta,
+//   zeta xi, xi eta zeta;
+// * the monomials are orthogonal under the element integral, so the strain
+//   energy splits into the constant gradient (an isotropic stress), three
+//   linear-gradient groups and one bilinear group, a few multiply-adds each;
+// * the modal forces return to the corners by the transposed transform.
+// About 180 FP64 operations instead of the 576 multiply-adds of the dense
+// 24x24 product. Corner arrays are indexed by bits dx + 2 dy + 4 dz; modal
+// index m = mx + 2 my + 4 mz is the monomial xi^mx eta^my zeta^mz.
+// The constants include the 1/64 of the two unnormalised transforms:
+//   L4 = 4 lam, M8 = 8 mu, M4 = 4 mu, A = 4 lam / 3, Cc = 4 mu / 3,
+//   K2 = 4 (lam + 4 mu) / 9, all / 64.
+struct H8Const {
+  double L4, M8, M4, A, Cc, K2;
+};
+__constant__ H8Const c_h8s;
+
+__host__ __device__ inline H8Const h8_const(double lam, double mu) {
+  const double q = 1.0 / 64.0;
+  return H8Const{4.0 * lam * q, 8.0 * mu * q, 4.0 * mu * q, (4.0 / 3.0) * lam * q,
+                 (4.0 / 3.0) * mu * q, (4.0 / 9.0) * (lam + 4.0 * mu) * q};
+}
+
+__host__ __device__ inline void h8_forces(const H8Const &k, double w, const double (&v)[8][3],
+                                          double (&f)[8][3]) {
+  double c[8][3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    double t[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i] = v[i][j];
+#pragma unroll
+    for (int b = 1; b < 8; b <<= 1)
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        if (!(i & b)) {
+          const double lo = t[i], hi = t[i + b];
+          t[i] = lo + hi;  // modal bit 0: the sum
+          t[i + b] = hi - lo;  // modal bit 1: + at the corner whose bit is 1
+        }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) c[i][j] = t[i];
+  }
+  const double L4 = w * k.L4, M8 = w * k.M8, M4 = w * k.M4;
+  const double A = w * k.A, Cc = w * k.Cc, K2 = w * k.K2;
+  // constant gradient: columns xi (m=1), eta (m=2), zeta (m=4)
+  const double *a = c[1], *b = c[2], *d = c[4];
+  const double ltr = L4 * (a[0] + b[1] + d[2]);
+  const double nx = fma(M8, a[0], ltr), ny = fma(M8, b[1], ltr), nz = fma(M8, d[2], ltr);
+  const double sxy = M4 * (a[1] + b[0]), sxz = M4 * (a[2] + d[0]), syz = M4 * (b[2] + d[1]);
+  // linear gradients: xi eta (m=3), eta zeta (m=6), zeta xi (m=5)
+  const double *p = c[3], *q = c[6], *r = c[5];
+  const double Te = A * (p[0] + q[2]), Tx = A * (p[1] + r[2]), Tz = A * (r[0] + q[1]);
+  const double W = (p[2] + r[1]) + q[0];
+  double F[8][3];
+  F[0][0] = F[0][1] = F[0][2] = 0.0;
+  F[1][0] = nx;  F[1][1] = sxy; F[1][2] = sxz;
+  F[2][0] = sxy; F[2][1] = ny;  F[2][2] = syz;
+  F[4][0] = sxz; F[4][1] = syz; F[4][2] = nz;
+  F[3][0] = fma(M4, p[0], Te); F[3][1] = fma(M4, p[1], Tx); F[3][2] = Cc * (W + p[2]);
+  F[6][0] = Cc * (W + q[0]);   F[6][1] = fma(M4, q[1], Tz); F[6][2] = fma(M4, q[2], Te);
+  F[5][0] = fma(M4, r[0], Tz); F[5][1] = Cc * (W + r[1]);   F[5][2] = fma(M4, r[2], Tx);
+  // bilinear: xi eta zeta (m=7)
+  F[7][0] = K2 * c[7][0]; F[7][1] = K2 * c[7][1]; F[7][2] = K2 * c[7][2];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    double t[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i] = F[i][j];
+#pragma unroll
+    for (int b2 = 1; b2 < 8; b2 <<= 1)
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        if (!(i & b2)) {
+          const double lo = t[i], hi = t[i + b2];
+          t[i] = lo - hi;      // corner bit 0: - the odd monomial
+          t[i + b2] = lo + hi;  // corner bit 1: +
+        }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) f[i][j] = t[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Element-centric plane march with the structured operator (matvec, direction
+// and residual modes; the element-block preconditioner keeps the dense
+// gather). A CTA owns a y-z tile of EY x EZ elements, one per thread, whose
+// origins are (y0 - 1 + ey, z0 - 1 + ez), and the (EY-1) x (EZ-1) nodes
+// (y0 + ey, z0 + ez) in it; it walks node planes xa .. xb-1 along x.
+// * Node planes are staged HE_DEPTH ahead by cp.async into a ring of raw
+//   slots: a slot holds one node plane's run (the values, and for the
+//   direction the previous direction too) and the weights of the element
+//   plane before it, one cp.async group per plane.
+// * Each thread reads its element's four corners in node plane x+1 from the
+//   ring, forming the direction p' = z + beta p there (a node's value is
+//   formed by each of its four elements, in the same arithmetic; the thread
+//   whose node it is stores it). Its corners in plane x are kept from the
+//   step before.
+// * A thread computes its element of element plane x (between node planes x
+//   and x+1) and keeps the two corners at its own node. The six other
+//   corners that nodes of the tile need are handed over in shared memory.
+// * A node then adds, in a fixed order, the dx = 0 corners of its four
+//   elements in element plane x and the dx = 1 corners carried from element
+//   plane x-1, and is finished. Each chunk of planes starts with element
+//   plane xa-1 (its dx = 1 corners only).
+// Two barriers per plane; no atomics; the summation order is fixed.
+// Shared memory (doubles): raw ring [HE_DEPTH][6 NS + HE_THREADS]; handover
+// [18][HE_THREADS]; NS = (EY + 1)(EZ + 1).
+// ---------------------------------------------------------------------------
+constexpr int HE_THREADS = 256;
+constexpr int HE_DEPTH = 3;
+constexpr int HE_KS = 6;  // staged values per thread and plane: 3 NS <= HE_KS * HE_THREADS
+__host__ __device__ inline int hex_elem_ns(int EY, int EZ) { return (EY + 1) * (EZ + 1); }
+__host__ __device__ inline int hex_elem_rs(int EY, int EZ) {
+  return 6 * hex_elem_ns(EY, EZ) + HE_THREADS;
+}
+__host__ __device__ inline size_t hex_elem_smem(int EY, int EZ) {
+  return (size_t)(HE_DEPTH * hex_elem_rs(EY, EZ) + 18 * HE_THREADS) * sizeof(double);
+}
+template <int N> __device__ __forceinline__ void cp_async_wait_pending() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int MODE, int PRE>
+__global__ void __launch_bounds__(HE_THREADS, 2)
+    k_hex_elem(Hex3Args a, int EY, int EZ, int tzc, int xc) {
+  static_assert(MODE != H3_BLOCK, "the element-block preconditioner uses the dense gather");
+  static_assert(HE_DEPTH >= 2, "the prologue waits for two staged planes");
+  PcgCtl *ctl = a.ctl;
+  if (MODE != H3_APPLY && ctl->status != TPO_SOLVE_RUNNING) return;
+  extern __shared__ double hs[];
+  const Hex3 g = a.g;
+  const int NS = hex_elem_ns(EY, EZ), RS = hex_elem_rs(EY, EZ);
+  const int RW = EZ + 1;                   // staged nodes per y-row
+  double *sring = hs;                      // raw ring
+  double *sx = sring + HE_DEPTH * RS;      // handover
+  const int ty = (int)blockIdx.x / tzc, tz = (int)blockIdx.x - ty * tzc;
+  const int y0 = ty * (EY - 1), z0 = tz * (EZ - 1);
+  const int xa = blockIdx.y * xc, xb = min(xa + xc, g.nx + 1);
+  const int t = threadIdx.x;
+  const bool el = t < EY * EZ;
+  const int ey = el ? t / EZ : 0, ez = el ? t - (t / EZ) * EZ : 0;
+  const int Y = y0 - 1 + ey, Z = z0 - 1 + ez;  // element origin
+  const bool eyz = el && Y >= 0 && Y < g.ny && Z >= 0 && Z < g.nz;
+  const int oy = y0 + ey, oz = z0 + ez;        // the node this thread finishes
+  const bool owner = el && ey < EY - 1 && ez < EZ - 1 && oy <= g.ny && oz <= g.nz;
+  const int64_t ny1 = g.ny + 1, nz1 = g.nz + 1;
+  const int64_t P1 = ny1 * nz1, P3 = 3 * P1;  // nodes, values per node plane
+  const int64_t own0 = (int64_t)oy * nz1 + oz;  // plane-relative index of the own node
+
+  bool first = true;
+  double beta = 0.0;
+  const double *pold = nullptr;
+  double *pnew = nullptr;
+  if (MODE == H3_DIR) {
+    first = ctl->first != 0;
+    beta = ctl->beta;
+    const bool odd = ctl->it & 1;
+    pold = odd ? a.pb : a.pa;
+    pnew = odd ? a.pa : a.pb;
+  }
+  const bool two = MODE == H3_DIR && !first;
+
+  // The staging pattern is the same in every plane: each thread's values as
+  // plane-relative offsets into the node arrays (-1 outside the grid). A
+  // plane has at most 2^29 nodes (grid <= 2^30 nodes, >= 2 planes), so the
+  // offsets fit 32 bits.
+  int goff[HE_KS];
+#pragma unroll
+  for (int k = 0; k < HE_KS; ++k) {
+    const int i = t + k * HE_THREADS;
+    const int li = i / 3;
+    const int iyl = li / RW, izl = li - iyl * RW;
+    const int y = y0 - 1 + iyl, z = z0 - 1 + izl;
+    goff[k] = (i < 3 * NS && y >= 0 && y <= g.ny && z >= 0 && z <= g.nz)
+                  ? 3 * (y * (int)nz1 + z) + (i - 3 * li)
+                  : -1;
+  }
+
+  auto slot_of = [&](int x) { return sring + ((x + 3 * HE_DEPTH) % HE_DEPTH) * RS; };
+  // raw run of node plane x and the weights of element plane x-1 -> its ring
+  // slot (3 values per node, as in memory), one cp.async group
+  auto issue = [&](int x) {
+    if (x <= xb) {  // planes past xb are not needed
+      double *sr = slot_of(x);
+      const bool xin = x >= 0 && x <= g.nx;
+      if (el) {
+        const int ex = x - 1;
+        if (eyz && ex >= 0 && ex < g.nx)
+          cp_async8(sr + 6 * NS + t, a.w + ((int64_t)ex * g.ny + Y) * g.nz + Z);
+        else
+          sr[6 * NS + t] = 0.0;
+      }
+      const double *bx = a.x + (int64_t)x * P3;
+      const double *bp = two ? pold + (int64_t)x * P3 : nullptr;
+#pragma unroll
+      for (int k = 0; k < HE_KS; ++k) {
+        const int i = t + k * HE_THREADS;
+        if (i >= 3 * NS) break;
+        if (xin && goff[k] >= 0) {
+          cp_async8(sr + i, bx + goff[k]);
+          if (two) cp_async8(sr + 3 * NS + i, bp + goff[k]);
+        } else {
+          sr[i] = 0.0;
+          if (two) sr[3 * NS + i] = 0.0;
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  // this thread's element corners (dy, dz) in node plane x, [dy + 2 dz][c],
+  // formed from the raw run; the direction's own node is stored once
+  auto corners = [&](int x, double (&q)[4][3]) {
+    const double *sr = slot_of(x) + 3 * (ey * RW + ez);
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const int o = 3 * (dy * RW + dz) + c;
+          q[dy + 2 * dz][c] = two ? fma(beta, sr[3 * NS + o], sr[o]) : sr[o];
+        }
+    if (MODE == H3_DIR && owner && x >= xa && x < xb) {
+      double *pn = pnew + (int64_t)x * P3 + 3 * own0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pn[c] = q[3][c];
+    }
+  };
+  auto weight_of = [&](int x) { return el ? slot_of(x)[6 * NS + t] : 0.0; };  // element plane x-1
+  // element forces from corners in planes x (lo) and x+1 (hi); the six
+  // corners other nodes take go to the handover arrays, the two at this
+  // thread's node stay: own[dx][c]
+  auto element = [&](const double (&lo)[4][3], const double (&hi)[4][3], double w,
+                     double (&own)[2][3]) {
+    double v[8][3], f[8][3];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        v[2 * k][c] = lo[k][c];      // bit dx = 0; k = dy + 2 dz -> bits 2 dy + 4 dz
+        v[2 * k + 1][c] = hi[k][c];  // dx = 1
+      }
+    h8_forces(c_h8s, w, v, f);
+#pragma unroll
+    for (int dx = 0; dx < 2; ++dx)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        sx[((0 * 2 + dx) * 3 + c) * HE_THREADS + t] = f[dx + 4][c];  // corner (0,1): node (ey-1, ez)
+        sx[((1 * 2 + dx) * 3 + c) * HE_THREADS + t] = f[dx + 2][c];  // corner (1,0): node (ey, ez-1)
+        sx[((2 * 2 + dx) * 3 + c) * HE_THREADS + t] = f[dx + 0][c];  // corner (0,0): node (ey-1, ez-1)
+        own[dx][c] = f[dx + 6][c];                                   // corner (1,1): this node
+      }
+  };
+  // this node's sum over its four elements of element plane x, corner dx
+  const int tA = (ey + 1) * EZ + ez, tB = ey * EZ + ez + 1, tC = (ey + 1) * EZ + ez + 1;
+  auto gather = [&](const double (&own)[2][3], int dx, double (&s)[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      s[c] = ((own[dx][c] + sx[((0 * 2 + dx) * 3 + c) * HE_THREADS + tA]) +
+              sx[((1 * 2 + dx) * 3 + c) * HE_THREADS + tB]) +
+             sx[((2 * 2 + dx) * 3 + c) * HE_THREADS + tC];
+  };
+
+  // prologue: node planes xa-1 .. xa-2+HE_DEPTH in flight; element plane
+  // xa-1 from planes xa-1 and xa, its dx = 1 corners carried into node plane
+  // xa. A ring slot is refilled (plane x + HE_DEPTH into the slot of plane
+  // x) once every thread has read plane x.
+  for (int k = 0; k < HE_DEPTH; ++k) issue(xa - 1 + k);
+  cp_async_wait_pending<HE_DEPTH - 2>();
+  __syncthreads();  // planes xa-1 and xa landed
+  double cur[4][3] = {}, nxt[4][3] = {}, own[2][3] = {}, carry[3] = {0.0, 0.0, 0.0};
+  unsigned fm = owner ? a.mask[(int64_t)xa * P1 + own0] : 0u;
+  if (el) {
+    corners(xa - 1, cur);
+    corners(xa, nxt);
+    element(cur, nxt, weight_of(xa), own);
+  }
+  __syncthreads();  // handover of element plane xa-1 complete; planes xa-1, xa read
+  if (owner) gather(own, 1, carry);
+  issue(xa - 1 + HE_DEPTH);
+  issue(xa + HE_DEPTH);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cur[k][c] = nxt[k][c];
+
+  double acc[2] = {0.0, 0.0};
+  for (int x = xa; x < xb; ++x) {
+    cp_async_wait_pending<HE_DEPTH - 1>();
+    __syncthreads();  // plane x+1 landed; every thread is done with the handover
+    // the mask of this thread's node in plane x+1, for the next step
+    const unsigned fm_next = (owner && x + 1 < xb) ? a.mask[(int64_t)(x + 1) * P1 + own0] : 0u;
+    if (el) {
+      corners(x + 1, nxt);
+      element(cur, nxt, weight_of(x + 1), own);
+    }
+    __syncthreads();  // handover of element plane x complete; plane x+1 read
+    issue(x + 1 + HE_DEPTH);
+    if (owner) {
+      double s0[3], s1[3];
+      gather(own, 0, s0);
+      gather(own, 1, s1);
+      double o[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        o[c] = carry[c] + s0[c];
+        carry[c] = s1[c];
+      }
+      // this node's own value in plane x: its element's corner (dx, dy, dz) = (0, 1, 1)
+      const double *self = cur[3];
+      const int64_t n = (int64_t)x * P1 + own0;
+      double *dst = a.out + 3 * n;
+      if (MODE == H3_APPLY || MODE == H3_DIR) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double ap = ((fm >> c) & 1u) ? self[c] : o[c];
+          dst[c] = ap;
+          acc[0] = fma(self[c], ap, acc[0]);
+        }
+      } else {  // H3_RES
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double ku = ((fm >> c) & 1u) ? self[c] : o[c];
+          const double r = a.f[3 * n + c] - ku;
+          dst[c] = r;
+          double zz = r;
+          if (PRE == TPO_PRECOND_JACOBI) {
+            zz = r / a.diag[3 * n + c];
+            a.z[3 * n + c] = zz;
+          }
+          acc[0] = fma(r, zz, acc[0]);
+          acc[1] = fma(r, r, acc[1]);
+        }
+      }
+    }
+    fm = fm_next;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) cur[k][c] = nxt[k][c];
+  }
+  cp_async_wait_all();
+  uint32_t *counter = MODE == H3_APPLY ? a.counter : &ctl->counter;
+  if (!grid_reduce<2>(acc, a.part, counter)) return;
+  if (threadIdx.x != 0) return;
+  if (MODE == H3_APPLY) {
+    if (a.pap_out) *a.pap_out = acc[0];
+  } else if (MODE == H3_DIR) {
+    const double pap = acc[0];
+    ctl->pap = pap;
+    ctl->first = 0;
+    if (!finite(pap)) ctl->status = TPO_SOLVE_NONFINITE;
+    else if (fabs(pap) < 1e-30) ctl->status = TPO_SOLVE_BREAKDOWN;  // solver.py:114-115
+    else ctl->alpha = ctl->rz / pap;                                  // solver.py:117
+  } else {
+    ctl->it = 0;
+    ctl->first = 1;
+    ctl->rz = acc[0];
+    ctl->rr = acc[1];
+    if (!finite(acc[0]) || !finite(acc[1])) ctl->status = TPO_SOLVE_NONFINITE;
   }
 }
 

@@ -7,6 +7,7 @@ namespace {
 
 bool g_have_stiffness3[kMaxDevices];
 double g_alpha_reg3[kMaxDevices];
+bool g_h8_structured[kMaxDevices];  // Ke is lam K_lam + mu K_mu: k_hex_elem applies it
 
 // Launch-size caps: grid-stride loops cover larger grids, and the grid
 // reductions read at most this many partials.
@@ -64,13 +65,56 @@ struct GatherPlan {
   dim3 grid;
   int xc = 0;
   size_t smem = 0;
+  // element-centric structured kernel (matvec, direction, residual)
+  bool elem = false;
+  dim3 egrid;
+  int ey = 0, ez = 0, tzc = 0, exc = 0;
+  size_t esmem = 0;
 };
+
+// Tiles of the element-centric kernel: EY x EZ elements (EY EZ <= HE_THREADS)
+// finish (EY-1) x (EZ-1) nodes; the shape that needs the fewest element slots
+// per plane to cover the (nely+1) x (nelz+1) nodes, then chunks of planes
+// for about one wave of resident CTAs.
+void elem_plan(const Hex3 &h, GatherPlan &p) {
+  int dev = 0;
+  if (current_device(&dev) || !g_h8_structured[dev]) return;
+  int64_t best = -1;
+  for (int ez = 3; ez <= HE_THREADS / 3; ++ez) {
+    const int ey = HE_THREADS / ez;
+    const int64_t tzc = (h.nz + 1 + ez - 2) / (ez - 1), tyc = (h.ny + 1 + ey - 2) / (ey - 1);
+    const int64_t cost = tzc * tyc * ey * ez;
+    if (tzc * tyc > kHexMaxCtas || hex_elem_smem(ey, ez) > kTileSmemMax ||
+        3 * hex_elem_ns(ey, ez) > HE_KS * HE_THREADS)
+      continue;
+    if (best < 0 || cost < best) {
+      best = cost;
+      p.ey = ey;
+      p.ez = ez;
+      p.tzc = (int)tzc;
+    }
+  }
+  if (best < 0) return;
+  const int64_t tiles = (int64_t)p.tzc * ((h.ny + 1 + p.ey - 2) / (p.ey - 1));
+  p.esmem = hex_elem_smem(p.ey, p.ez);
+  const int64_t planes = (int64_t)h.nx + 1;
+  const int64_t wave =
+      (int64_t)resident_ctas(k_hex_elem<H3_DIR, 0>, HE_THREADS, p.esmem) * sm_count();
+  int64_t chunks = std::max<int64_t>(1, wave / tiles);
+  chunks = std::min<int64_t>(std::min<int64_t>(chunks, planes), kHexMaxCtas / tiles);
+  const int64_t xc = (planes + chunks - 1) / chunks;
+  chunks = (planes + xc - 1) / xc;
+  p.egrid = dim3((unsigned)tiles, (unsigned)chunks, 1);
+  p.exc = (int)xc;
+  p.elem = true;
+}
 
 GatherPlan gather_plan(const Hex3 &h) {
   GatherPlan p;
   const int64_t P = (int64_t)(h.ny + 1) * (h.nz + 1);
   const int64_t cpp = (P + HT_THREADS - 1) / HT_THREADS;
   const size_t smem = hex_tile_smem(h.nz);
+  elem_plan(h, p);
   if (smem > kTileSmemMax || cpp > kHexMaxCtas) {
     p.grid = hex_gather_grid(h);
     return p;
@@ -90,6 +134,16 @@ GatherPlan gather_plan(const Hex3 &h) {
 
 template <int MODE, int PRE>
 int launch_gather(const GatherPlan &p, const Hex3Args &a, cudaStream_t st) {
+  if constexpr (MODE != H3_BLOCK) {
+    if (p.elem) {
+      if (p.esmem > 48 * 1024)
+        TPO_CK(cudaFuncSetAttribute(k_hex_elem<MODE, PRE>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.esmem));
+      k_hex_elem<MODE, PRE><<<p.egrid, HE_THREADS, p.esmem, st>>>(a, p.ey, p.ez, p.tzc, p.exc);
+      TPO_CK_LAUNCH();
+      return TPO_OK;
+    }
+  }
   if (p.tile) {
     if (p.smem > 48 * 1024)
       TPO_CK(cudaFuncSetAttribute(k_hex_tile<MODE, PRE>,
@@ -275,6 +329,44 @@ tpo_grid flat_oc_grid(const tpo_grid3 *g) {
   return f;
 }
 
+// Ke as lam K_lam + mu K_mu, the unit-cube isotropic H8 operator
+// (h8_forces): least squares over the 576 entries, accepted when every entry
+// agrees to 1e-12 of the largest. Otherwise the dense gathers apply Ke.
+bool h8_fit(const double ke[576], double *lam, double *mu) {
+  static const int dxyz[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                 {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};  // reference order
+  int bit_of[8];
+  for (int r = 0; r < 8; ++r) bit_of[r] = dxyz[r][0] + 2 * dxyz[r][1] + 4 * dxyz[r][2];
+  std::vector<double> kl(576), km(576);
+  const H8Const cl = h8_const(1.0, 0.0), cm = h8_const(0.0, 1.0);
+  for (int col = 0; col < 24; ++col) {
+    double v[8][3] = {}, fl[8][3], fm[8][3];
+    v[bit_of[col / 3]][col % 3] = 1.0;
+    h8_forces(cl, 1.0, v, fl);
+    h8_forces(cm, 1.0, v, fm);
+    for (int row = 0; row < 24; ++row) {
+      kl[row * 24 + col] = fl[bit_of[row / 3]][row % 3];
+      km[row * 24 + col] = fm[bit_of[row / 3]][row % 3];
+    }
+  }
+  double a11 = 0, a12 = 0, a22 = 0, b1 = 0, b2 = 0, kmax = 0;
+  for (int i = 0; i < 576; ++i) {
+    a11 += kl[i] * kl[i];
+    a12 += kl[i] * km[i];
+    a22 += km[i] * km[i];
+    b1 += kl[i] * ke[i];
+    b2 += km[i] * ke[i];
+    kmax = std::max(kmax, std::fabs(ke[i]));
+  }
+  const double det = a11 * a22 - a12 * a12;
+  if (!(det > 0.0) || !(kmax > 0.0)) return false;
+  *lam = (b1 * a22 - b2 * a12) / det;
+  *mu = (a11 * b2 - a12 * b1) / det;
+  for (int i = 0; i < 576; ++i)
+    if (std::fabs(ke[i] - (*lam * kl[i] + *mu * km[i])) > 1e-12 * kmax) return false;
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -289,6 +381,12 @@ int tpo_set_stiffness3(const double ke[576], const double ke_inv[576], double al
       return fail(TPO_ERR_ARGS, "non-finite stiffness entry %d", i);
   TPO_CK(cudaMemcpyToSymbol(c_ke3, ke, sizeof(double) * 576));
   TPO_CK(cudaMemcpyToSymbol(c_kinv3, ke_inv, sizeof(double) * 576));
+  double lam = 0.0, mu = 0.0;
+  g_h8_structured[dev] = h8_fit(ke, &lam, &mu);
+  if (g_h8_structured[dev]) {
+    const H8Const k = h8_const(lam, mu);
+    TPO_CK(cudaMemcpyToSymbol(c_h8s, &k, sizeof(H8Const)));
+  }
   g_alpha_reg3[dev] = alpha_reg;
   g_have_stiffness3[dev] = true;
   return TPO_OK;
