@@ -1568,8 +1568,6 @@ static __device__ __align__(256) unsigned char g_sens_scratch[TPO_SENS_NOALLOC_S
 static constexpr size_t kSensTicketBytes = 256;
 static constexpr size_t kSensMaxPartials =
     (TPO_SENS_NOALLOC_SCRATCH - kSensTicketBytes) / sizeof(double);
-static void *g_sens_scratch_addr[kMaxDevices];
-static std::mutex g_sens_scratch_mu;
 
 int tpo_sensitivity_noalloc(const tpo_grid *g, const double *rho_phys, const double *u,
                             double *dc, double *compliance_out, tpo_stream s) {
@@ -1587,16 +1585,10 @@ int tpo_sensitivity_noalloc(const tpo_grid *g, const double *rho_phys, const dou
                 "grid %dx%d needs %zu partial sums; the fixed scratch holds %zu "
                 "(ceil(nely/128)*ceil(nelx/16) must be <= %zu)",
                 g->nelx, g->nely, nb, kSensMaxPartials, kSensMaxPartials);
-  void *base;
-  {
-    std::lock_guard<std::mutex> lk(g_sens_scratch_mu);
-    if (!g_sens_scratch_addr[dev]) {
-      void *ptr = nullptr;
-      TPO_CK(cudaGetSymbolAddress(&ptr, g_sens_scratch));
-      g_sens_scratch_addr[dev] = ptr;
-    }
-    base = g_sens_scratch_addr[dev];
-  }
+  // looked up on every call (a host-side query, nothing allocated), so the
+  // address always belongs to the device's current context
+  void *base = nullptr;
+  TPO_CK(cudaGetSymbolAddress(&base, g_sens_scratch));
   cudaStream_t st = static_cast<cudaStream_t>(s);
   SumCtl *ctl = static_cast<SumCtl *>(base);
   double *part = reinterpret_cast<double *>(static_cast<unsigned char *>(base) + kSensTicketBytes);
