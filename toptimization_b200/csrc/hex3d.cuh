@@ -955,6 +955,59 @@ __global__ void __launch_bounds__(H3_FLAT)
   if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
 }
 
+// The same update with 16-byte loads and stores, two DOFs per thread and
+// step (every array 16-byte aligned; the host checks). An odd last DOF is
+// taken by the thread that would hold its pair.
+template <int PRE>
+__global__ void __launch_bounds__(H3_FLAT)
+    k_hex_update2(int64_t ndof, double *__restrict__ u, double *__restrict__ r,
+                  const double *__restrict__ pa, const double *__restrict__ pb,
+                  const double *__restrict__ ap, const double *__restrict__ diag,
+                  double *__restrict__ z, double *part, PcgCtl *ctl) {
+  if (ctl->status != TPO_SOLVE_RUNNING) return;
+  const double alpha = ctl->alpha;
+  const double *__restrict__ p = (ctl->it & 1) ? pa : pb;  // written by this iteration's direction
+  double acc[2] = {0.0, 0.0};
+  auto one = [&](double uu, double pp, double aa, double rr, double dd, double &uo, double &ro,
+                 double &zo) {
+    uo = fma(alpha, pp, uu);
+    ro = fma(-alpha, aa, rr);
+    if (PRE != TPO_PRECOND_BLOCK_JACOBI) {
+      zo = PRE == TPO_PRECOND_JACOBI ? ro / dd : ro;
+      acc[0] = fma(ro, zo, acc[0]);
+      acc[1] = fma(ro, ro, acc[1]);
+    }
+  };
+  const int64_t npair = ndof / 2;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= npair;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (k < npair) {
+      const double2 uu = reinterpret_cast<const double2 *>(u)[k];
+      const double2 pp = reinterpret_cast<const double2 *>(p)[k];
+      const double2 aa = reinterpret_cast<const double2 *>(ap)[k];
+      const double2 rr = reinterpret_cast<const double2 *>(r)[k];
+      const double2 dd = PRE == TPO_PRECOND_JACOBI ? reinterpret_cast<const double2 *>(diag)[k]
+                                                   : make_double2(1.0, 1.0);
+      double2 uo, ro, zo;
+      one(uu.x, pp.x, aa.x, rr.x, dd.x, uo.x, ro.x, zo.x);
+      one(uu.y, pp.y, aa.y, rr.y, dd.y, uo.y, ro.y, zo.y);
+      reinterpret_cast<double2 *>(u)[k] = uo;
+      reinterpret_cast<double2 *>(r)[k] = ro;
+      if (PRE == TPO_PRECOND_JACOBI) reinterpret_cast<double2 *>(z)[k] = zo;
+    } else if (ndof & 1) {  // k == npair: the odd last DOF
+      const int64_t i = ndof - 1;
+      double uo, ro, zo;
+      one(u[i], p[i], ap[i], r[i], PRE == TPO_PRECOND_JACOBI ? diag[i] : 1.0, uo, ro, zo);
+      u[i] = uo;
+      r[i] = ro;
+      if (PRE == TPO_PRECOND_JACOBI) z[i] = zo;
+    }
+  }
+  if (PRE == TPO_PRECOND_BLOCK_JACOBI) return;
+  if (!grid_reduce<2>(acc, part, &ctl->counter)) return;
+  if (threadIdx.x == 0) finish_update(ctl, acc[0], acc[1]);
+}
+
 // SIMP scales s = e_min + rho^p (1 - e_min) (reference fem/kernels.py:92) and,
 // for the element-block preconditioner, w = s / max(s, alpha)^2
 // (preconditioner.py:128-130).

@@ -191,10 +191,17 @@ int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const do
   const double tol_sq = (c->tol * fn) * (c->tol * fn);
   const dim3 gg = hex_gather_grid(h);
   const GatherPlan gp = gather_plan(h);
-  // the update streams 8 vectors: one wave of resident CTAs, grid-stride
+  // the update streams 8 vectors: one wave of resident CTAs, grid-stride;
+  // 16-byte accesses when every array allows them
+  const bool vec = aligned(u, 16) && aligned(w.r, 16) && aligned(w.pa, 16) &&
+                   aligned(w.pb, 16) && aligned(w.ap, 16) && aligned(w.diag, 16) &&
+                   aligned(w.z, 16);
   const dim3 fg = flat_grid(nd, H3_FLAT,
                             std::min(kHexMaxCtas, resident_ctas(k_hex_update<PRE>, H3_FLAT, 0) *
                                                       sm_count()));
+  const dim3 fg2 = flat_grid(nd / 2 + 1, H3_FLAT,
+                             std::min(kHexMaxCtas, resident_ctas(k_hex_update2<PRE>, H3_FLAT, 0) *
+                                                       sm_count()));
   // warm start from u with its fixed DOFs zeroed, else from zero (solver.py:52-57)
   if (c->warm_start) {
     k_hex_zero_fixed<<<hex_flat_grid(nn), H3_FLAT, 0, st>>>(nn, fixed, u);
@@ -256,8 +263,12 @@ int pcg3(const tpo_grid3 *g, const tpo_solve_cfg *c, const double *rho, const do
     if (r) return r;
     if (ev) TPO_CK(cudaEventRecord(ev[1], st));
     if (ev) TPO_CK(cudaEventRecord(ev[2], st));
-    k_hex_update<PRE><<<fg, H3_FLAT, 0, st>>>(nd, u, w.r, w.pa, w.pb, w.ap, w.diag, w.z, w.part,
-                                              w.ctl);
+    if (vec)
+      k_hex_update2<PRE><<<fg2, H3_FLAT, 0, st>>>(nd, u, w.r, w.pa, w.pb, w.ap, w.diag, w.z,
+                                                  w.part, w.ctl);
+    else
+      k_hex_update<PRE><<<fg, H3_FLAT, 0, st>>>(nd, u, w.r, w.pa, w.pb, w.ap, w.diag, w.z,
+                                                w.part, w.ctl);
     TPO_CK_LAUNCH();
     if (PRE == TPO_PRECOND_BLOCK_JACOBI && (r = launch_gather<H3_BLOCK, 0>(gp, b, st))) return r;
     if (ev) TPO_CK(cudaEventRecord(ev[3], st));
