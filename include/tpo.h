@@ -366,7 +366,11 @@ typedef struct tpo_grid3 {
 /* 24x24 H8 stiffness (row-major, DOFs [x,y,z] per corner in mesh.py:87-96
  * order), its regularised inverse (Ke + alpha I)^-1 and alpha (reference
  * material.py:89-171, fem/fields.py:133-143), into constant memory of the
- * CURRENT device. Must be called once per device before any tpo3_* kernel. */
+ * CURRENT device. Must be called once per device before any tpo3_* kernel.
+ * When ke is the isotropic unit-cube H8 stiffness (lam K_lam + mu K_mu, every
+ * entry within 1e-12 of the largest), the stiffness applications use a
+ * structured element operator with the fitted lam, mu; any other ke is applied
+ * as the dense 24x24 matrix. Both give the same operator to rounding. */
 int tpo_set_stiffness3(const double ke[576], const double ke_inv[576], double alpha_reg);
 
 /* ap = K(rho) p, identity rows at fixed DOFs; *pap_out (device, nullable) =
