@@ -329,6 +329,12 @@ int tpo_batch_add(tpo_batch *b, const tpo_batch_design *d, const double *f, cons
                   void *design_ws, size_t design_ws_bytes, tpo_stream s, int32_t *slot_out);
 /* Releases a slot (its workspace may be reused once this returns). */
 int tpo_batch_remove(tpo_batch *b, int32_t slot);
+/* The design in `slot` takes only the PCG steps i of each loop body with
+ * i % period == 0 (default 1: every step). The design computes the same
+ * iterates, only spread over more loop bodies; a server gives large designs
+ * a longer period so that a loop body of small ones does not wait on them.
+ * Synchronous; takes effect from the next launch. No reference counterpart. */
+int tpo_batch_set_step_period(tpo_batch *b, int32_t slot, int32_t period);
 int tpo_batch_set_tiles(tpo_batch *b, int32_t stencil_cols, int32_t update_cols);
 /* One OC iteration of every active design; blocks until it is done. With
  * use_graph the iteration is one CUDA graph launch. */

@@ -149,15 +149,21 @@ def test_rounds_and_oc_iterations_agree(tpo_built):
     b.close()
 
 
-def test_served_results_equal_alone(tpo_built):
+@pytest.mark.parametrize("step_elems", [65536, 1500])
+def test_served_results_equal_alone(tpo_built, step_elems):
     """Each request's result in the served stream (others arriving and
-    leaving around it) is bit-identical to the same request run alone."""
+    leaving around it) is bit-identical to the same request run alone, with
+    every step (alone) and, for step_elems 1500, served with step periods of
+    2 to 16 (size-aware steps)."""
     from toptimization_b200.serve import Server, poisson_stream
     reqs = poisson_stream(6, rate=200.0, seed=3, nelx_range=(64, 160), max_iter=4)
-    srv = Server(max_slots=8, keep_density=True)
+    srv = Server(max_slots=8, keep_density=True, size_steps=True, size_step_elems=step_elems)
+    periods = [srv.step_period(r.problem) for r in reqs]
     rep = srv.serve(reqs)
     srv.close()
     assert len(rep.completions) == 6 and rep.peak_resident >= 2
+    if step_elems < 65536:
+        assert max(periods) >= 4
     for c in rep.completions:
         alone = Batch(1)
         s = alone.add(reqs[c.rid].problem)

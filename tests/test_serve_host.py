@@ -16,6 +16,9 @@ class FakeBatch:
         self.need = {}
         self.closed = False
 
+    def set_step_period(self, slot, period):
+        assert slot in self.progress and period >= 1
+
     def add(self, pr, max_iter=None, tag=None):
         slot = next(i for i in range(self.max) if i not in self.progress)
         self.progress[slot] = 0
@@ -77,3 +80,17 @@ def test_summary_percentiles():
     s = serve.ServeReport(cs).summary()
     assert s["designs_per_s"] == pytest.approx(100 / 100.0)
     assert s["p50_s"] == pytest.approx(50.5) and s["p99_s"] == pytest.approx(99.01)
+
+
+def test_step_period_is_a_power_of_two_bounded_by_the_round():
+    from toptimization_b200.serve import step_period
+    assert step_period(1000, 32, 65536) == 1
+    assert step_period(65536, 32, 65536) == 1
+    assert step_period(2 * 65536, 32, 65536) == 2
+    assert step_period(3 * 65536, 32, 65536) == 2
+    assert step_period(1024 * 1024, 32, 65536) == 16
+    assert step_period(1 << 30, 32, 65536) == 32
+    assert step_period(1 << 30, 4, 65536) == 4
+    for n in (1, 7000, 130000, 500000, 4000000):
+        p = step_period(n, 32, 65536)
+        assert p & (p - 1) == 0 and 1 <= p <= 32

@@ -146,6 +146,7 @@ _SIGS = {
                               c_size_t, c_void_p, _PI]),
     "tpo_batch_remove": (c_int, [c_void_p, c_int32]),
     "tpo_batch_set_tiles": (c_int, [c_void_p, c_int32, c_int32]),
+    "tpo_batch_set_step_period": (c_int, [c_void_p, c_int32, c_int32]),
     "tpo_batch_oc_iteration": (c_int, [c_void_p, c_void_p]),
     "tpo_batch_round": (c_int, [c_void_p, c_int32, c_void_p]),
     "tpo_batch_states": (c_int, [c_void_p, c_int32, _PI, _PI]),

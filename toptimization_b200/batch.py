@@ -123,6 +123,11 @@ class Batch:
         _lib.check(self.lib.tpo_batch_remove(self.handle, int(slot)))
         del self.slots[slot]
 
+    def set_step_period(self, slot: int, period: int) -> None:
+        """The design takes every `period`-th PCG step of a loop body (1: all):
+        the same iterates, spread over more bodies."""
+        _lib.check(self.lib.tpo_batch_set_step_period(self.handle, int(slot), int(period)))
+
     def set_tiles(self, stencil_cols: int, update_cols: int) -> None:
         _lib.check(self.lib.tpo_batch_set_tiles(self.handle, int(stencil_cols), int(update_cols)))
 

@@ -42,7 +42,9 @@ enum BPhase { PH_PRE = 0, PH_SOLVE = 1, PH_POST = 2 };
 struct BDesign {
   int nx, ny, P, active;       // active: OC iterations remain
   int it, max_it, R, max_cg;   // OC iterations done / requested, filter radius, PCG cap
-  int max_outer, phase, pad0, pad1;  // phase: BPhase
+  int max_outer, phase;        // phase: BPhase
+  int period;                  // takes the PCG steps i of a loop body with i % period == 0 (0, 1: all)
+  int pad1;
   double e_min, pen, volfrac, move, rmin, tol;  // tol: early stop on change (0: none)
   double tol_sq, rupd2;        // PCG stop (true residual) and replacement thresholds
   // compact fields, reference numbering
@@ -154,10 +156,11 @@ __global__ void __launch_bounds__(TS_THREADS) kb_resx(const BJob *jobs, int nj, 
 }
 
 template <int PRE>
-__global__ void __launch_bounds__(TS_THREADS) kb_dir(const BJob *jobs, int nj, const BDesign *ds) {
+__global__ void __launch_bounds__(TS_THREADS) kb_dir(const BJob *jobs, int nj, const BDesign *ds,
+                                                     int step) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
-  if (!D.active) return;
+  if (!D.active || (D.period > 1 && step % D.period != 0)) return;
   TsArgs a{};
   a.nx = D.nx;
   a.ny = D.ny;
@@ -189,10 +192,10 @@ __global__ void __launch_bounds__(UF_THREADS) kb_pre(const BJob *jobs, int nj, c
 
 template <int PRE>
 __global__ void __launch_bounds__(UF_THREADS) kb_update(const BJob *jobs, int nj,
-                                                        const BDesign *ds) {
+                                                        const BDesign *ds, int step) {
   const BJob &J = find_job(jobs, nj);
   const BDesign &D = ds[J.slot];
-  if (!D.active) return;
+  if (!D.active || (D.period > 1 && step % D.period != 0)) return;
   UpdArgs a{};
   a.nx = D.nx;
   a.ny = D.ny;

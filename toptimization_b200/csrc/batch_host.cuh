@@ -251,10 +251,10 @@ int batch_body(tpo_batch *b, cudaStream_t st, cudaGraphConditionalHandle h, int 
   TPO_CK_LAUNCH();
   for (int i = 0; i < steps; ++i) {
     kb_dir<PRE><<<b->nctas[BK_STENCIL], TS_THREADS, SMEM_D, st>>>(
-        jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs);
+        jobs_of(b, BK_STENCIL), b->njobs[BK_STENCIL], b->d_designs, i);
     TPO_CK_LAUNCH();
     kb_update<PRE><<<b->nctas[BK_UPDATE], UF_THREADS, 0, st>>>(
-        jobs_of(b, BK_UPDATE), b->njobs[BK_UPDATE], b->d_designs);
+        jobs_of(b, BK_UPDATE), b->njobs[BK_UPDATE], b->d_designs, i);
     TPO_CK_LAUNCH();
   }
   if (!cond) return TPO_OK;
@@ -597,6 +597,15 @@ int tpo_batch_remove(tpo_batch *b, int32_t slot) {
   b->h_status[2 * slot + 1] = 0;
   while (b->n_slots > 0 && !b->used[b->n_slots - 1]) --b->n_slots;
   b->dirty = true;
+  return TPO_OK;
+}
+
+int tpo_batch_set_step_period(tpo_batch *b, int32_t slot, int32_t period) {
+  if (!b || slot < 0 || slot >= b->max_designs || !b->used[slot])
+    return fail(TPO_ERR_ARGS, "no design in slot %d", slot);
+  if (period < 1) return fail(TPO_ERR_ARGS, "the step period must be >= 1");
+  b->rec[slot].period = period;
+  TPO_CK(cudaMemcpy(&b->d_designs[slot].period, &period, sizeof(int), cudaMemcpyHostToDevice));
   return TPO_OK;
 }
 

@@ -8,7 +8,17 @@ its state then stays resident on the device until its last OC iteration.
 Every round advances all resident designs together (`Batch.round`), each at
 its own OC iteration, warm-starting every PCG from the design's previous
 displacement. Requests that arrive while others are on the GPU join at the
-next round. No reference counterpart: the reference solves one problem per
+next round.
+
+Size-aware steps (size_steps=True; off by default, since they trade
+throughput for the small designs' latency): a design of E elements takes
+every p-th PCG step of a
+round, p the largest power of two <= E / E_ref (at most the round's steps),
+E_ref the larger of size_step_elems and the smallest resident design. Each
+resident design then costs about the same GPU time per step, so small
+designs are not paced by the largest ones; when the small ones have left,
+the large ones return to every step. A design's iterates, and so its
+result, do not depend on p. No reference counterpart: the reference solves one problem per
 process (`src/toptimization/cli.py:22-144`).
 
 The one-at-a-time baseline serves the same stream with plain FP64 solves
@@ -88,14 +98,26 @@ def poisson_stream(n: int, rate: float, seed: int = 0, nelx_range=(64, 1024),
     return [Request(i, float(t[i]), ps[i]) for i in range(n)]
 
 
+def step_period(n_elem: int, round_steps: int, elems: int) -> int:
+    """Largest power of two p <= n_elem / elems, 1 <= p <= round_steps."""
+    p = 1
+    while 2 * p <= round_steps and 2 * p * elems <= n_elem:
+        p *= 2
+    return p
+
+
 class Server:
     """Continuous-batching server over one `Batch`."""
 
     def __init__(self, hbm_budget: float = 150e9, max_slots: int = 256, *,
                  preconditioner: str = "nodal_block_jacobi", use_graph: bool = True,
                  tiles: tuple[int, int] | None = None, round_steps: int = 32,
-                 rounds_per_check: int = 4, keep_density: bool = False, device=None):
+                 rounds_per_check: int = 4, keep_density: bool = False,
+                 size_steps: bool = False, size_step_elems: int = 65536, device=None):
         self.budget = float(hbm_budget)
+        self.round_steps = int(round_steps)
+        self.size_steps = bool(size_steps)
+        self.size_step_elems = int(size_step_elems)
         self.batch = Batch(max_slots, preconditioner=preconditioner, use_graph=use_graph,
                            tiles=tiles, round_steps=round_steps, device=device)
         self.rounds_per_check = int(rounds_per_check)
@@ -106,6 +128,7 @@ class Server:
         b = self.batch
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         resident: dict[int, tuple[Request, float, int]] = {}
+        periods: dict[int, int] = {}
         used = 0
         rep = ServeReport([])
         t0 = time.perf_counter()
@@ -122,6 +145,8 @@ class Server:
             if not resident:
                 time.sleep(max(0.0, pending[0].arrival - now))
                 continue
+            if self.size_steps:
+                self._set_periods(resident, periods)
             rep.peak_resident = max(rep.peak_resident, len(resident))
             rep.peak_bytes = max(rep.peak_bytes, used)
             # admission and completions are checked between groups of rounds;
@@ -137,10 +162,24 @@ class Server:
                 rep.completions.append(Completion(req.rid, req.arrival, adm, t, int(it[slot]),
                                                   float(hist["compliance"][-1]), rho))
                 b.remove(slot)
+                periods.pop(slot, None)
                 used -= fp
         rep.wall = time.perf_counter() - t0
         rep.completions.sort(key=lambda c: c.rid)
         return rep
+
+    def step_period(self, pr: Problem, ref: int | None = None) -> int:
+        return step_period(pr.n_elem, self.round_steps,
+                           max(self.size_step_elems, ref or 0))
+
+    def _set_periods(self, resident: dict, periods: dict) -> None:
+        """Step periods relative to the smallest resident design."""
+        ref = min(req.problem.n_elem for req, _, _ in resident.values())
+        for slot, (req, _, _) in resident.items():
+            p = self.step_period(req.problem, ref)
+            if periods.get(slot, 1) != p:
+                self.batch.set_step_period(slot, p)
+            periods[slot] = p
 
     def close(self) -> None:
         self.batch.close()
@@ -173,4 +212,4 @@ def serve_one_at_a_time(requests: list[Request], precision: str = "fp64",
 
 
 __all__ = ["Request", "Completion", "ServeReport", "Server", "poisson_stream",
-           "serve_one_at_a_time"]
+           "serve_one_at_a_time", "step_period"]
